@@ -1,0 +1,117 @@
+/*
+ * wtd.h — C ABI of the B200 TD-(A)SLDA/BdG step library (one library per W-SLDA project,
+ * built from the project's predefines.h and problem-definition.h).
+ *
+ * This is the fused entry surface.  It replaces, as one stream-ordered unit, the sequence the
+ * reference's host driver issues per time step through its C ABI
+ *   hpc-engine/pca.c:1401-1571 (cpca.c:1262-, ccpca.c:1137-) calling
+ *   abm_step1 / abm_step4          hpc-engine/tdwslda_ode_integrator.h:106, :195
+ *   normalize_wf                   hpc-engine/pca_kernels.cu:955
+ *   compute_derivatives / _laplace hpc-engine/pca_derivative.cu:217, :332
+ *   calculate_densities            hpc-engine/pca_dens.cu:220
+ *   density_caculate_tau           hpc-engine/pca_dens.cu:300
+ *   compute_potentials             hpc-engine/pca_kernels.cu:81
+ *   apply_hamiltonian              hpc-engine/pca_kernels.cu:674
+ *   compute_energy                 hpc-engine/pca_kernels.cu:211
+ * and the constant setters memcopy_const / memcopy_const_params / memcopy_const_sclgth /
+ * memcopy_extra_data (hpc-engine/wslda_cuda_utils.h:47-105).
+ *
+ * Conventions (kept from the reference):
+ *  - N = NX (1D), NX*NY (2D), NX*NY*NZ (3D); x is the slowest index.
+ *  - states: 2*nwf*N complex numbers [u_0..u_{nwf-1}, v_0..v_{nwf-1}], interleaved (re, im)
+ *    doubles on the host, as cufftDoubleComplex / double complex in the reference.
+ *  - densities: 12*N doubles [nu (complex), rho_a, tau_a, j_a_x, j_a_y, j_a_z,
+ *    rho_b, tau_b, j_b_x, j_b_y, j_b_z] (hpc-engine/pca_dens.cu:233-243).
+ *  - potentials: 12*N doubles [V_a, V_b, Delta (complex), alpha_a, alpha_b, A_a_xyz, A_b_xyz]
+ *    (hpc-engine/wslda_potdens.c:44-70).
+ *  - energy: TDWSLDAITEMS = 11 doubles [E_kin, E_pot, E_pair, E_curr, E_ext_V, E_ext_Delta,
+ *    E_ext_v, N_a, N_b, L_za, L_zb] (hpc-engine/pca_settings.h:143-158).
+ *  - return value 0 = success; nonzero = error (see wtd_error_string).  No call exits the
+ *    process.
+ *  - every call is ordered on the context's CUDA stream; calls that return host data
+ *    synchronise before returning.
+ */
+#ifndef WTD_H
+#define WTD_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct wtd_ctx wtd_ctx;
+
+/* precision forms */
+#define WTD_FP64 0        /* states, history, FFT and H psi in FP64 (drop-in form) */
+#define WTD_MIXED_H64 1   /* states, FFT and H psi in FP32; ABM history/P stored in FP64 */
+#define WTD_MIXED_H32 2   /* states, history, FFT and H psi in FP32; ABM sums, norms, densities FP64 */
+
+/* error codes */
+#define WTD_OK 0
+#define WTD_ERR_ARG -1
+#define WTD_ERR_CUDA -2
+#define WTD_ERR_UNSUPPORTED -3
+#define WTD_ERR_STATE -4
+#define WTD_ERR_NOMEM -5
+
+/* lattice and build facts of this library: dims[3], numel, codedim, scheme history length,
+ * functional id (111 SLDA, 112 ASLDA, 113 BDG, 114 CUSTOMEDF), const-mass flag */
+int wtd_info(int *dims, int *numel, int *codedim, int *nhist, int *functional, int *const_mass);
+/* device bytes a context of nwf states in the given precision needs */
+size_t wtd_device_bytes(int nwf, int precision);
+
+int wtd_create(wtd_ctx **ctx, int nwf, int precision, int device);
+int wtd_destroy(wtd_ctx *ctx);
+const char *wtd_error_string(int code);
+
+/* constants: replaces memcopy_const (wslda_cuda_utils.h:50), memcopy_const_params (:80),
+ * memcopy_const_sclgth (:90), memcopy_extra_data (:44) */
+int wtd_set_constants(wtd_ctx *ctx, double mu_a, double mu_b, double ec, double t0, double dt, double kF);
+int wtd_set_params(wtd_ctx *ctx, const double *params /* MAX_USER_PARAMS */);
+int wtd_set_sclgth(wtd_ctx *ctx, double a);
+int wtd_set_extra_data(wtd_ctx *ctx, const void *host, size_t bytes);
+/* user host hook process_params from problem-definition.h (pca.c:903) */
+int wtd_process_params(wtd_ctx *ctx, double *params, double *kF, double *mu);
+
+/* data in: occupations f_n (pca.c:837) and, for 1D/2D, per-state plane-wave ky, kz and
+ * degeneracy cnt (NULL = 0, 0, 1) */
+int wtd_upload_states(wtd_ctx *ctx, const double *host_states);
+int wtd_upload_potentials(wtd_ctx *ctx, const double *host_pots);
+int wtd_upload_occupations(wtd_ctx *ctx, const double *fbeta, const double *kky, const double *kkz, const int *cnt);
+/* reference ABM history f1..fq (hpc-engine/tdwslda_checkpoint.c:223-364 layout, f1 newest);
+ * slot in [0, q) */
+int wtd_upload_history(wtd_ctx *ctx, int slot, const double *host);
+int wtd_download_history(wtd_ctx *ctx, int slot, double *host);
+
+/* initial measurement (pca.c:939-958): normalise, all densities, tau; zero ABM history */
+int wtd_initial_measurement(wtd_ctx *ctx, int it0);
+/* nsteps ABM steps forming one measurement block (pca.c:1401-1571): tau and j are formed on
+ * the block's last step (constant mass) or on every step (variable mass) */
+int wtd_steps(wtd_ctx *ctx, int nsteps);
+/* compute_energy (hpc-engine/tdwslda_energy_generic.h:21-111) into host[11] */
+int wtd_energy(wtd_ctx *ctx, double *host11);
+int wtd_sync(wtd_ctx *ctx);
+int wtd_time_index(wtd_ctx *ctx);
+
+int wtd_download_states(wtd_ctx *ctx, double *host_states);
+int wtd_download_densities(wtd_ctx *ctx, double *host_dens);
+int wtd_download_potentials(wtd_ctx *ctx, double *host_pots);
+/* <psi_n|H|psi_n> dV of the last H application (left in d_workarea by the reference) */
+int wtd_download_qpe(wtd_ctx *ctx, double *host_qpe);
+
+/* device pointers (for callers that keep data on the GPU): states, densities, potentials */
+int wtd_device_pointers(wtd_ctx *ctx, void **states, double **dens, double **pots);
+/* CUDA stream the context orders its work on (cudaStream_t) */
+void *wtd_stream(wtd_ctx *ctx);
+/* kernels launched by this context since creation (the fused passes and O(N) kernels) */
+long long wtd_launch_count(wtd_ctx *ctx);
+/* device timing of the two fused stream passes (CUDA events on the context stream around each
+ * launch): enable, then read the summed milliseconds and launch counts since the last read */
+int wtd_set_timing(wtd_ctx *ctx, int on);
+int wtd_pass_times(wtd_ctx *ctx, double *ms_pass_a, double *ms_pass_b, int *count_a, int *count_b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

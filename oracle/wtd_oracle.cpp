@@ -1,0 +1,890 @@
+/*
+ * ORACLE — TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU (FP64, host C++) restatement of one real-time step of W-SLDA's TD-(A)SLDA/BdG engine,
+ * used by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg to check and time
+ * the CUDA library.  It is never linked into, imported by or called from the product path.
+ *
+ * Built once per project, like the reference (`make -C oracle PROJECT=<name>`): the project's
+ * predefines.h and problem-definition.h are compiled in through oracle_surface.h, so the user
+ * hooks (v_ext, delta_ext, scattering_length, CUSTOMEDF kernels) run here unchanged.
+ *
+ * Every routine restates the reference function cited beside it, in the same arithmetic order
+ * where the order matters for rounding (ABM combinations, the 1e4 DENS_FACTOR_M scaling of the
+ * density weights).  FFTs are this file's own mixed-radix Cooley-Tukey transform with the
+ * cuFFT/FFTW sign convention (forward e^{-2 pi i k n / N}, inverse unnormalised).
+ *
+ * Parity pins: tests/golden/ holds outputs of the reference's own CUDA kernels
+ * (oracle/ref_harness.cu linked against hpc-engine/*.cu) on small seeded cases; the oracle
+ * is checked against them in tests/test_oracle_golden.py.
+ */
+#include "oracle_surface.h"
+#include "predefines.h"
+#include "wtd_settings.h"
+static double dc_params[MAX_USER_PARAMS];
+#include "oracle_edf.h"
+#include "problem-definition.h"
+
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#if defined(ENABLE_V_EXT)
+#define ORC_U_EXT(ix, iy, iz, it, spin) v_ext(ix, iy, iz, it, spin, dc_params, dc_extra_data_size, dc_extra_data)
+#else
+#define ORC_U_EXT(ix, iy, iz, it, spin) 0.0
+#endif
+#if defined(ENABLE_DELTA_EXT)
+#define ORC_D_EXT(ix, iy, iz, it, d) delta_ext(ix, iy, iz, it, d, dc_params, dc_extra_data_size, dc_extra_data)
+#else
+#define ORC_D_EXT(ix, iy, iz, it, d) Complex(0.0, 0.0)
+#endif
+
+namespace orc {
+
+static const int N = WTD_NUMEL;
+static const int AXN[3] = {NX, (CODEDIM >= 2) ? NY : 1, (CODEDIM >= 3) ? NZ : 1};
+static const double AXL[3] = {LX, LY, LZ};
+static const int NHIST = WTD_NHIST;
+
+static int S = 0;             /* number of (u,v) quasiparticle states */
+static int it_global = 0;
+static std::vector<Complex> y, fk[5], ddx, ddy, ddz, dlap, dalap;
+static std::vector<double> dens, pots, fb, kky, kkz, qpe, work;
+static std::vector<int> cnt;
+static std::vector<unsigned char> extra;
+static int last_gradients = 0;
+
+/* point coordinates of linear index i (pca_macro.h:134-160) */
+static inline void decode(int i, int &ix, int &iy, int &iz)
+{
+#if CODEDIM == 3
+    ix = i / (NY * NZ); int r = i - ix * NY * NZ; iy = r / NZ; iz = r - iy * NZ;
+#elif CODEDIM == 2
+    ix = i / NY; iy = i - ix * NY; iz = 0;
+#else
+    ix = i; iy = 0; iz = 0;
+#endif
+}
+
+/* ----------------------------------------------------------------------------------------
+ * FFT: recursive mixed-radix decimation in time, radices 4, 2, 3, then generic DFT.
+ * sign = -1 forward, +1 inverse (unnormalised), as cuFFT CUFFT_FORWARD / CUFFT_INVERSE.
+ * --------------------------------------------------------------------------------------*/
+struct Plan1D {
+    int n = 0;
+    std::vector<Complex> wf, wi; /* e^{-2 pi i j/n}, e^{+2 pi i j/n} */
+};
+static Plan1D plans[3];
+
+static void make_plan(Plan1D &p, int n)
+{
+    p.n = n;
+    p.wf.resize(n); p.wi.resize(n);
+    for (int j = 0; j < n; j++) {
+        /* exact symmetric angle reduction keeps the table to libm accuracy */
+        long double a = 2.0L * (long double)M_PI * (long double)j / (long double)n;
+        double c = (double)std::cos(a), s = (double)std::sin(a);
+        p.wf[j] = Complex(c, -s);
+        p.wi[j] = Complex(c, s);
+    }
+}
+
+static void fft_rec(const Complex *in, Complex *out, int n, int stride, const Complex *w, int wstep)
+{
+    if (n == 1) { out[0] = in[0]; return; }
+    int r = (n % 4 == 0) ? 4 : (n % 2 == 0) ? 2 : (n % 3 == 0) ? 3 : n;
+    int m = n / r;
+    if (r == n) { /* generic DFT */
+        for (int k = 0; k < n; k++) {
+            Complex s(0.0, 0.0);
+            for (int q = 0; q < n; q++) s += in[q * stride] * w[((long)q * k % n) * wstep];
+            out[k] = s;
+        }
+        return;
+    }
+    for (int q = 0; q < r; q++) fft_rec(in + q * stride, out + q * m, m, stride * r, w, wstep * r);
+    Complex t[4];
+    std::vector<Complex> tmp(n);
+    for (int k = 0; k < m; k++) {
+        for (int q = 0; q < r; q++) t[q] = out[q * m + k] * w[(long)q * k * wstep];
+        for (int j = 0; j < r; j++) {
+            Complex s(0.0, 0.0);
+            for (int q = 0; q < r; q++) s += t[q] * w[((long)q * j * m % n) * wstep];
+            tmp[k + j * m] = s;
+        }
+    }
+    for (int i = 0; i < n; i++) out[i] = tmp[i];
+}
+
+/* in-place FFT of one lattice field (row-major, x slowest) along every lattice axis */
+static void fftn(Complex *a, int sign)
+{
+    std::vector<Complex> line, res;
+    int dims = CODEDIM;
+    for (int ax = 0; ax < dims; ax++) {
+        int n = AXN[ax];
+        if (n == 1) continue;
+        int inner = 1;
+        for (int b = ax + 1; b < dims; b++) inner *= AXN[b];
+        int outer = N / (n * inner);
+        line.resize(n); res.resize(n);
+        const Complex *w = (sign < 0) ? plans[ax].wf.data() : plans[ax].wi.data();
+        for (int o = 0; o < outer; o++)
+            for (int in = 0; in < inner; in++) {
+                Complex *base = a + (size_t)o * n * inner + in;
+                for (int j = 0; j < n; j++) line[j] = base[(size_t)j * inner];
+                fft_rec(line.data(), res.data(), n, 1, w, 1);
+                for (int j = 0; j < n; j++) base[(size_t)j * inner] = res[j];
+            }
+    }
+}
+
+/* wave number of index i on axis ax (pca_derivative.cu:152-160) */
+static inline double kval(int ax, int i)
+{
+    int n = AXN[ax];
+    return (i < n / 2) ? 2. * M_PI / AXL[ax] * (double)i : 2. * M_PI / AXL[ax] * (double)(i - n);
+}
+
+/* compute_derivatives for one complex field (pca_derivative.cu:139-277): d/dx_d with the
+ * Nyquist mode zeroed, laplacian without; 1/N folded into the k factors. Any output may be
+ * null. */
+static void derivs_one(const Complex *f, Complex *dx, Complex *dy, Complex *dz, Complex *lap)
+{
+    std::vector<Complex> F(f, f + N);
+    fftn(F.data(), -1);
+    Complex *outs[3] = {dx, dy, dz};
+    std::vector<Complex> G(N);
+    for (int d = 0; d < CODEDIM; d++) {
+        if (!outs[d]) continue;
+        for (int i = 0; i < N; i++) {
+            int c[3]; decode(i, c[0], c[1], c[2]);
+            double k = kval(d, c[d]) / N;
+            if (c[d] == AXN[d] / 2) k = 0.0;
+            G[i] = Complex(-k * F[i].imag(), k * F[i].real());
+        }
+        fftn(G.data(), +1);
+        std::copy(G.begin(), G.end(), outs[d]);
+    }
+    if (lap) {
+        for (int i = 0; i < N; i++) {
+            int c[3]; decode(i, c[0], c[1], c[2]);
+            double k2 = 0.0;
+            for (int d = 0; d < CODEDIM; d++) { double k = kval(d, c[d]); k2 += k * k; }
+            k2 = -1.0 * k2 / N;
+            G[i] = Complex(k2 * F[i].real(), k2 * F[i].imag());
+        }
+        fftn(G.data(), +1);
+        std::copy(G.begin(), G.end(), lap);
+    }
+}
+
+/* laplacian / d f_d/dx_d of real fields (pca_derivative.cu:490-700, D2Z/Z2D); the complex
+ * transform of a real field gives the same real result. */
+static void lap_real(const double *f, double *out)
+{
+    std::vector<Complex> F(N), L(N);
+    for (int i = 0; i < N; i++) F[i] = Complex(f[i], 0.0);
+    derivs_one(F.data(), nullptr, nullptr, nullptr, L.data());
+    for (int i = 0; i < N; i++) out[i] = L[i].real();
+}
+static void dcomp_real(const double *f, int d, double *out)
+{
+    std::vector<Complex> F(N), D(N);
+    for (int i = 0; i < N; i++) F[i] = Complex(f[i], 0.0);
+    Complex *o[3] = {nullptr, nullptr, nullptr};
+    o[d] = D.data();
+    derivs_one(F.data(), o[0], o[1], o[2], nullptr);
+    for (int i = 0; i < N; i++) out[i] = D[i].real();
+}
+
+/* ---------------------------------------------------------------------------------------
+ * field views
+ * -------------------------------------------------------------------------------------*/
+static inline Complex *U(std::vector<Complex> &a, int n) { return a.data() + (size_t)n * N; }
+static inline Complex *V(std::vector<Complex> &a, int n) { return a.data() + (size_t)S * N + (size_t)n * N; }
+static wslda_density dens_view(double *d)
+{
+    wslda_density r;
+    r.nx = NX; r.ny = AXN[1]; r.nz = AXN[2]; r.datadim = CODEDIM; r.blocklength = N;
+    r.nu = (Complex *)d;
+    r.rho_a = d + 2 * N; r.tau_a = d + 3 * N; r.j_a_x = d + 4 * N; r.j_a_y = d + 5 * N; r.j_a_z = d + 6 * N;
+    r.rho_b = d + 7 * N; r.tau_b = d + 8 * N; r.j_b_x = d + 9 * N; r.j_b_y = d + 10 * N; r.j_b_z = d + 11 * N;
+    return r;
+}
+static wslda_potential pots_view(double *d)
+{
+    wslda_potential r;
+    r.nx = NX; r.ny = AXN[1]; r.nz = AXN[2]; r.datadim = CODEDIM; r.blocklength = N;
+    r.V_a = d; r.V_b = d + N; r.delta = (Complex *)(d + 2 * N); r.alpha_a = d + 4 * N; r.alpha_b = d + 5 * N;
+    r.A_a_x = d + 6 * N; r.A_a_y = d + 7 * N; r.A_a_z = d + 8 * N;
+    r.A_b_x = d + 9 * N; r.A_b_y = d + 10 * N; r.A_b_z = d + 11 * N;
+    r.mu = nullptr;
+    return r;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * ABM predictor / corrector (tdwslda_ode_integrator.h:26-220)
+ * -------------------------------------------------------------------------------------*/
+static void abm_step1(Complex *yv, Complex *f1, Complex *f2, Complex *f3, Complex *f4, Complex *f5)
+{
+    const Complex dti(0.0, -1.0 * dc_dt);
+    const size_t M = (size_t)2 * S * N;
+#pragma omp parallel for
+    for (long i = 0; i < (long)M; i++) {
+        Complex y0 = yv[i];
+#if INTEGRATION_SCHEME == AB3AM4
+        Complex a = f1[i], b = f2[i], c = f3[i];
+        yv[i] = y0 + dti * (a * (23. / 12.) - b * (16. / 12.) + c * (5. / 12.));
+        f3[i] = y0 + dti * (a * (19. / 24.) - b * (5. / 24.) + c * (1. / 24.));
+#elif INTEGRATION_SCHEME == AB4AM5
+        Complex a = f1[i], b = f2[i], c = f3[i], d = f4[i];
+        yv[i] = y0 + dti * (a * (55. / 24.) - b * (59. / 24.) + c * (37. / 24.) - d * (9. / 24.));
+        f4[i] = y0 + dti * (a * (646. / 720.) - b * (264. / 720.) + c * (106. / 720.) - d * (19. / 720.));
+#else
+        Complex a = f1[i], b = f2[i], c = f3[i], d = f4[i], e = f5[i];
+        yv[i] = y0 + dti * (a * (1901. / 720.) - b * (2774. / 720.) + c * (2616. / 720.) - d * (1274. / 720.) + e * (251. / 720.));
+        f5[i] = y0 + dti * (a * (646. / 720.) - b * (264. / 720.) + c * (106. / 720.) - d * (19. / 720.));
+#endif
+    }
+}
+static void abm_step4(const Complex *hy, Complex *yout, const Complex *flast)
+{
+    const Complex dti(0.0, -1.0 * dc_dt);
+#if INTEGRATION_SCHEME == AB3AM4
+    const double c = 9. / 24.;
+#else
+    const double c = 251. / 720.;
+#endif
+    const size_t M = (size_t)2 * S * N;
+#pragma omp parallel for
+    for (long i = 0; i < (long)M; i++) yout[i] = dti * hy[i] * c + flast[i];
+}
+
+/* normalize_wf (pca_kernels.cu:913-976): psi_n /= sqrt(sum_x (|u|^2+|v|^2) dV) */
+static void normalize(std::vector<Complex> &w)
+{
+#pragma omp parallel for
+    for (int n = 0; n < S; n++) {
+        Complex *u = U(w, n), *v = V(w, n);
+        double s = 0.0;
+        for (int i = 0; i < N; i++) s += (std::norm(u[i]) + std::norm(v[i])) * WTD_DV;
+        double c = 1.0 / std::sqrt(s);
+        for (int i = 0; i < N; i++) { u[i] *= c; v[i] *= c; }
+    }
+}
+
+/* derivatives of all 2S component fields (compute_derivatives / compute_laplace) */
+static void derivatives(std::vector<Complex> &w, int grads)
+{
+#pragma omp parallel for schedule(dynamic)
+    for (long m = 0; m < 2L * S; m++) {
+        size_t o = (size_t)m * N;
+        if (grads)
+            derivs_one(w.data() + o, ddx.data() + o, CODEDIM >= 2 ? ddy.data() + o : nullptr,
+                       CODEDIM >= 3 ? ddz.data() + o : nullptr, dlap.data() + o);
+        else
+            derivs_one(w.data() + o, nullptr, nullptr, nullptr, dlap.data() + o);
+    }
+}
+
+/* calculate_densities (pca_dens.cu:13-198; cpca_dens.cu:14-140; ccpca_dens.cu:14-140) */
+static void calculate_densities(std::vector<Complex> &w, int grads)
+{
+    wslda_density D = dens_view(dens.data());
+    const double DF = 10000.;
+#pragma omp parallel for
+    for (int i = 0; i < N; i++) {
+        double na = 0, nb = 0, taua = 0, taub = 0, jax = 0, jay = 0, jaz = 0, jbx = 0, jby = 0, jbz = 0;
+        Complex nu(0.0, 0.0);
+        for (int n = 0; n < S; n++) {
+            double fbEn = fb[n] * DF, fbmEn = DF - fbEn;
+            double wcnt = 1.0, kp2 = 0.0;
+#if CODEDIM == 2
+            double kz = kkz[n];
+            kp2 = kz * kz;
+            wcnt = (std::fabs(kz) < 1.0e-12) ? 1.0 : 2.0;
+#ifdef USE_CUBIC_CUTOFF
+            if (std::fabs(kz + M_PI / DZ) < 1.0e-12) wcnt = 1.0;
+#endif
+#elif CODEDIM == 1
+            kp2 = kkz[n] * kkz[n] + kky[n] * kky[n];
+            wcnt = (double)cnt[n];
+#endif
+            Complex u = U(w, n)[i], v = V(w, n)[i];
+            na += std::norm(u) * fbEn * wcnt;
+            nb += std::norm(v) * fbmEn * wcnt;
+            nu += u * std::conj(v) * (fbmEn - fbEn) / 2.0 * wcnt;
+            if (grads) {
+                Complex lu = U(dlap, n)[i], lv = V(dlap, n)[i];
+                taua += (std::conj(u) * (lu - u * kp2)).real() * fbEn * wcnt;
+                taub += (std::conj(v) * (lv - v * kp2)).real() * fbmEn * wcnt;
+                jax += (std::conj(u) * U(ddx, n)[i]).imag() * fbEn * wcnt;
+                jbx -= (std::conj(v) * V(ddx, n)[i]).imag() * fbmEn * wcnt;
+#if CODEDIM >= 2
+                jay += (std::conj(u) * U(ddy, n)[i]).imag() * fbEn * wcnt;
+                jby -= (std::conj(v) * V(ddy, n)[i]).imag() * fbmEn * wcnt;
+#endif
+#if CODEDIM >= 3
+                jaz += (std::conj(u) * U(ddz, n)[i]).imag() * fbEn * wcnt;
+                jbz -= (std::conj(v) * V(ddz, n)[i]).imag() * fbmEn * wcnt;
+#endif
+            }
+        }
+        const double L = WTD_LPERP;
+        D.rho_a[i] = na / DF / L; D.rho_b[i] = nb / DF / L;
+        D.tau_a[i] = taua / DF / L; D.tau_b[i] = taub / DF / L;
+        D.nu[i] = nu / DF / L;
+        D.j_a_x[i] = jax / DF / L; D.j_a_y[i] = jay / DF / L; D.j_a_z[i] = jaz / DF / L;
+        D.j_b_x[i] = jbx / DF / L; D.j_b_y[i] = jby / DF / L; D.j_b_z[i] = jbz / DF / L;
+    }
+}
+
+/* density_caculate_tau (pca_dens.cu:275-338): tau = max(0, lap(rho)/2 - tau_tmp) */
+static void density_tau()
+{
+    wslda_density D = dens_view(dens.data());
+    std::vector<double> lr(N);
+    double *rho[2] = {D.rho_b, D.rho_a}, *tau[2] = {D.tau_b, D.tau_a};
+    for (int s = 0; s < 2; s++) {
+        lap_real(rho[s], lr.data());
+        for (int i = 0; i < N; i++) {
+            double t = 0.5 * lr[i] - tau[s][i];
+            if (t < 0.0) t = 0.0;
+            tau[s][i] = t;
+        }
+    }
+}
+
+/* ---------------------------------------------------------------------------------------
+ * compute_potentials (pca_kernels.cu:81-94 -> tdwslda_functionals.h)
+ * -------------------------------------------------------------------------------------*/
+#if FUNCTIONAL == SLDA || FUNCTIONAL == ASLDA
+/* tdwslda_functionals.h:47-306 */
+static void potentials_point(int it, int i, wslda_density Dn, wslda_potential P, double cccoeff)
+{
+    using namespace oedf;
+    int ix, iy, iz; decode(i, ix, iy, iz);
+    double Va_const = ORC_U_EXT(ix, iy, iz, it, SPINA);
+    double Vb_const = ORC_U_EXT(ix, iy, iz, it, SPINB);
+    double na = Dn.rho_a[i], nb = Dn.rho_b[i];
+    double t1 = pol(na, nb);
+    double aplus = alpha_plus(t1);
+    double dam_a, dam_b, dap_a, dap_b;
+#ifdef CURRENT_CORRECTIONS
+    double aminus = alpha_minus(t1);
+    double t2 = alpha(t1), t3 = alpha(-t1);
+    P.alpha_a[i] = t2; P.alpha_b[i] = t3;
+    double *Aa[3] = {P.A_a_x, P.A_a_y, P.A_a_z}, *Ab[3] = {P.A_b_x, P.A_b_y, P.A_b_z};
+    double *ja[3] = {Dn.j_a_x, Dn.j_a_y, Dn.j_a_z}, *jb[3] = {Dn.j_b_x, Dn.j_b_y, Dn.j_b_z};
+    double t4 = p_reg(na) * cccoeff;
+    for (int d = 0; d < CODEDIM; d++) Aa[d][i] = (t4 == 0.0) ? 0.0 : t4 * (1. - t2) * ja[d][i] / na;
+    t4 = p_reg(nb) * cccoeff;
+    for (int d = 0; d < CODEDIM; d++) Ab[d][i] = (t4 == 0.0) ? 0.0 : t4 * (1. - t3) * jb[d][i] / nb;
+#endif
+#ifdef FAST_CONST_EFFECTIVE_MASS_MODE
+    dam_a = dam_b = dap_a = dap_b = 0.0;
+#else
+    {
+        double ta = Dn.tau_a[i], tb = Dn.tau_b[i];
+        double tm = ta - tb;
+        dam_a = oedf::dam_da(na, nb); dam_b = oedf::dam_db(na, nb);
+        Va_const += dam_a * tm / 2.0; Vb_const += dam_b * tm / 2.0;
+        double tp = ta + tb;
+        dap_a = oedf::dap_da(na, nb); dap_b = oedf::dap_db(na, nb);
+        Va_const += dap_a * tp / 2.0; Vb_const += dap_b * tp / 2.0;
+    }
+#endif
+    Va_const += dD_da(na, nb);
+    Vb_const += dD_db(na, nb);
+#ifdef CURRENT_CORRECTIONS
+    {
+        double jx = Dn.j_a_x[i], kx = Dn.j_b_x[i];
+        double jy = (CODEDIM >= 2) ? Dn.j_a_y[i] : 0.0, ky = (CODEDIM >= 2) ? Dn.j_b_y[i] : 0.0;
+        double jz = (CODEDIM >= 3) ? Dn.j_a_z[i] : 0.0, kz = (CODEDIM >= 3) ? Dn.j_b_z[i] : 0.0;
+        double t7 = p_reg(na) * cccoeff;
+        if (t7 != 0.0) {
+            t7 = t7 * (jx * jx + jy * jy + jz * jz) / (2.0 * na);
+            Va_const += ((aplus + aminus - 1.0) / na - (dap_a + dam_a)) * t7;
+            Va_const -= cccoeff * dp_reg(na) * (aplus + aminus - 1.0) * (jx * jx + jy * jy + jz * jz) / (2.0 * na);
+            Vb_const -= (dap_b + dam_b) * t7;
+        }
+        t7 = p_reg(nb) * cccoeff;
+        if (t7 != 0.0) {
+            t7 = t7 * (kx * kx + ky * ky + kz * kz) / (2.0 * nb);
+            Va_const -= (dap_a - dam_a) * t7;
+            Vb_const += ((aplus - aminus - 1.0) / nb - (dap_b - dam_b)) * t7;
+            Vb_const -= cccoeff * dp_reg(nb) * (aplus - aminus - 1.0) * (kx * kx + ky * ky + kz * kz) / (2.0 * nb);
+        }
+    }
+#endif
+    double c1 = dap_a / aplus, c2 = dap_b / aplus;
+    double c3 = dtC_da(na, nb) / aplus, c4 = dtC_db(na, nb) / aplus;
+    double tC = tildeC(na, nb);
+    double Va = P.V_a[i], Vb = P.V_b[i];
+    Complex lnu = Dn.nu[i], ldelta(0.0, 0.0), Zone(1.0, 0.0), p0, kc, wz;
+#ifdef INCLUDE_MF_CORRECTION_FROM_REG_SCHEME
+    double lkF = std::pow(3.0 * M_PI * M_PI * (na + nb), 1.0 / 3.0);
+#endif
+    for (int k = 0; k < UD_SCITERS; k++) {
+        double t7 = (dc_mu_a - Va + dc_mu_b - Vb) / 2.0;
+        p0 = std::sqrt(Complex(2.0 * t7 / aplus, 0.0));
+        if (p0.imag() < 0.) p0 *= -1.;
+#ifdef USE_CUBIC_CUTOFF
+        kc = Complex(M_PI / DX, 0.0);
+#else
+        kc = std::sqrt(Complex(2.0 * (dc_ec + t7) / aplus, 0.0));
+        if (kc.imag() < 0.) kc *= -1.;
+#endif
+        wz = std::log((kc + p0) / (kc - p0));
+        if (wz.imag() < 0.) wz += Complex(0.0, 2. * M_PI);
+        wz = kc * REG_COEFF_R0 * (1. - (p0 / kc) * REG_COEFF_R1 * wz);
+        wz = Zone * aplus / (Zone * tC - wz);
+        ldelta = lnu * (-1.0 * wz.real());
+        double t6 = (std::conj(ldelta) * lnu).real();
+        double tn = std::norm(ldelta);
+        double Vanew = Va_const - c1 * t6 - c3 * tn;
+        double Vbnew = Vb_const - c2 * t6 - c4 * tn;
+#ifdef INCLUDE_MF_CORRECTION_FROM_REG_SCHEME
+        {
+            double bcoeff = (p0 / (lkF + 1.0e-12)).real();
+            double lx = bcoeff * lkF * DX / M_PI;
+            if (wz.real() < -1.0e-10 && lx > 1.0e-10) {
+                double L0 = bcoeff * REG_COEFF_R0 / lx * (1.0 - REG_COEFF_R1 * lx * std::log((1.0 + lx) / (1.0 - lx)));
+                double dL0 = (-2. * bcoeff * REG_COEFF_R0 * REG_COEFF_R1) / (1. - lx * lx) - bcoeff * REG_COEFF_R0 / lx / lx;
+                double dLdn = (lkF / (3. * (na + nb) * aplus)) * (L0 + dL0 * bcoeff * DX * lkF / M_PI);
+                Vanew += dLdn * tn;
+                Vbnew += dLdn * tn;
+            }
+        }
+#endif
+        Va = UD_MIX_COEFF * Vanew + (1.0 - UD_MIX_COEFF) * Va;
+        Vb = UD_MIX_COEFF * Vbnew + (1.0 - UD_MIX_COEFF) * Vb;
+    }
+    P.V_a[i] = Va; P.V_b[i] = Vb; P.delta[i] = ldelta;
+}
+#elif FUNCTIONAL == BDG
+/* tdwslda_functionals.h:373-452 */
+static void potentials_point(int it, int i, wslda_density Dn, wslda_potential P, double cccoeff)
+{
+    int ix, iy, iz; decode(i, ix, iy, iz);
+    double Va = ORC_U_EXT(ix, iy, iz, it, SPINA);
+    double Vb = ORC_U_EXT(ix, iy, iz, it, SPINB);
+    double aplus = 0.5 * (P.alpha_a[i] + P.alpha_b[i]);
+    double t5 = 1.0 / (4.0 * M_PI * scattering_length(ix, iy, iz, it, dc_params, dc_extra_data_size, dc_extra_data) * aplus);
+    Complex lnu = Dn.nu[i], Zone(1.0, 0.0), p0, kc, wz;
+#ifdef INCLUDE_MF_CORRECTION_FROM_REG_SCHEME
+    double nab = Dn.rho_a[i] + Dn.rho_b[i];
+    double lkF = std::pow(3.0 * M_PI * M_PI * nab, 1.0 / 3.0);
+#endif
+    double t7 = (dc_mu_a - P.V_a[i] + dc_mu_b - P.V_b[i]) / 2.0;
+    p0 = std::sqrt(Complex(2.0 * t7, 0.0));
+    if (p0.imag() < 0.) p0 *= -1.;
+#ifdef USE_CUBIC_CUTOFF
+    kc = Complex(M_PI / DX, 0.0);
+#else
+    kc = std::sqrt(Complex(2.0 * (dc_ec + t7), 0.0));
+    if (kc.imag() < 0.) kc *= -1.;
+#endif
+    wz = std::log((kc + p0) / (kc - p0));
+    if (wz.imag() < 0.) wz += Complex(0.0, 2. * M_PI);
+    wz = kc * REG_COEFF_R0 / aplus * (1. - (p0 / kc) * REG_COEFF_R1 * wz);
+    wz = Zone / (Zone * t5 - wz);
+    Complex ldelta = lnu * (-1.0 * wz.real());
+#ifdef INCLUDE_MF_CORRECTION_FROM_REG_SCHEME
+    {
+        double bcoeff = (p0 / (lkF + 1.0e-12)).real();
+        double lx = bcoeff * lkF * DX / M_PI;
+        if (wz.real() < -1.0e-10 && lx > 1.0e-10) {
+            double L0 = bcoeff * REG_COEFF_R0 / lx * (1.0 - REG_COEFF_R1 * lx * std::log((1.0 + lx) / (1.0 - lx)));
+            double dL0 = (-2. * bcoeff * REG_COEFF_R0 * REG_COEFF_R1) / (1. - lx * lx) - bcoeff * REG_COEFF_R0 / lx / lx;
+            double dLdn = (lkF / (3. * nab * aplus)) * (L0 + dL0 * bcoeff * DX * lkF / M_PI);
+            double tn = std::norm(ldelta);
+            Va += dLdn * tn;
+            Vb += dLdn * tn;
+        }
+    }
+#endif
+    P.V_a[i] = Va; P.V_b[i] = Vb; P.delta[i] = ldelta;
+}
+#endif
+
+static void compute_potentials(int it)
+{
+    wslda_density Dn = dens_view(dens.data());
+    wslda_potential P = pots_view(pots.data());
+#if FUNCTIONAL == CUSTOMEDF
+    blockIdx.x = 0; blockDim.x = 1;
+    for (int i = 0; i < N; i++) { threadIdx.x = i; tdwslda_compute_potentials(it, Dn, P, 1.0); }
+#else
+#pragma omp parallel for
+    for (int i = 0; i < N; i++) potentials_point(it, i, Dn, P, 1.0);
+#endif
+#ifdef ENABLE_MODIFY_POTENTIALS
+    blockIdx.x = 0; blockDim.x = 1;
+    for (int i = 0; i < N; i++) { threadIdx.x = i; modify_potentials(it, Dn, P); }
+#endif
+}
+
+/* multiply_wf_by_alpha + compute_laplace (pca_kernels.cu:981-1026, pca.c:1455-1456) */
+static void alpha_laplace(std::vector<Complex> &w)
+{
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+    wslda_potential P = pots_view(pots.data());
+#pragma omp parallel for schedule(dynamic)
+    for (long m = 0; m < 2L * S; m++) {
+        const double *al = (m < S) ? P.alpha_a : P.alpha_b;
+        std::vector<Complex> t(N);
+        const Complex *src = w.data() + (size_t)m * N;
+        for (int i = 0; i < N; i++) t[i] = src[i] * al[i];
+        derivs_one(t.data(), nullptr, nullptr, nullptr, dalap.data() + (size_t)m * N);
+    }
+#else
+    (void)w;
+#endif
+}
+
+/* apply_hamiltonian (pca_kernels.cu:233-495, 674-848; cpca_kernels.cu:231-490;
+ * ccpca_kernels.cu:209-448): out = (H - <H>) w.  out may alias the laplacian buffer. */
+static void apply_hamiltonian(int it, std::vector<Complex> &w, Complex *out)
+{
+    wslda_potential P = pots_view(pots.data());
+#ifdef CURRENT_CORRECTIONS
+    std::vector<double> dA[2][3], lal[2];
+#endif
+#if !defined(FAST_CONST_EFFECTIVE_MASS_MODE)
+    std::vector<double> lapal_a(N), lapal_b(N);
+    lap_real(P.alpha_a, lapal_a.data());
+    lap_real(P.alpha_b, lapal_b.data());
+#endif
+#ifdef CURRENT_CORRECTIONS
+    double *Aa[3] = {P.A_a_x, P.A_a_y, P.A_a_z}, *Ab[3] = {P.A_b_x, P.A_b_y, P.A_b_z};
+    for (int d = 0; d < CODEDIM; d++) {
+        dA[0][d].resize(N); dA[1][d].resize(N);
+        dcomp_real(Aa[d], d, dA[0][d].data());
+        dcomp_real(Ab[d], d, dA[1][d].data());
+    }
+#endif
+    std::vector<Complex> Dt(N);
+    for (int i = 0; i < N; i++) {
+        int ix, iy, iz; decode(i, ix, iy, iz);
+        Complex D = P.delta[i];
+#ifdef ENABLE_DELTA_EXT
+        D = D + ORC_D_EXT(ix, iy, iz, it, D);
+#endif
+        Dt[i] = D;
+    }
+#pragma omp parallel for
+    for (int n = 0; n < S; n++) {
+        double kp2 = 0.0;
+#if CODEDIM == 2
+        kp2 = kkz[n] * kkz[n];
+#elif CODEDIM == 1
+        kp2 = kky[n] * kky[n] + kkz[n] * kkz[n];
+#endif
+        for (int i = 0; i < N; i++) {
+            Complex tu = U(w, n)[i], tv = V(w, n)[i];
+            Complex lu = U(dlap, n)[i], lv = V(dlap, n)[i];
+            double Va = P.V_a[i], Vb = P.V_b[i];
+            Complex D = Dt[i];
+            Complex u(0.0, 0.0), v(0.0, 0.0);
+            double cja = 0.0, cjb = 0.0;
+#ifdef BDG_MODE
+            double p = 0.5 * kp2;
+            u += tu * Complex(Va - dc_mu_a + p, cja);
+            v -= tv * Complex(Vb - dc_mu_b + p, -1.0 * cjb);
+            u += tv * D;
+            v += tu * std::conj(D);
+            u += lu * (-0.5);
+            v -= lv * (-0.5);
+#else
+#ifdef FAST_CONST_EFFECTIVE_MASS_MODE
+            double aa = P.alpha_a[i] * -0.5, ab = P.alpha_b[i] * -0.5;
+            double ja = -1.0 * aa * kp2, jb = -1.0 * ab * kp2;
+#else
+            double aa = P.alpha_a[i] * -0.25, ab = P.alpha_b[i] * -0.25;
+            double na = 0.25 * lapal_a[i], nb = 0.25 * lapal_b[i];
+            double ja = -2.0 * aa * kp2, jb = -2.0 * ab * kp2;
+#endif
+#ifdef CURRENT_CORRECTIONS
+            Complex ga[3], gb[3];
+            for (int d = 0; d < 3; d++) { ga[d] = Complex(0, 0); gb[d] = Complex(0, 0); }
+            for (int d = 0; d < CODEDIM; d++) {
+                cja += -0.5 * dA[0][d][i];
+                cjb += -0.5 * dA[1][d][i];
+                ga[d] += Complex(0.0, -1. * Aa[d][i]);
+                gb[d] += Complex(0.0, 1. * Ab[d][i]);
+            }
+#endif
+            u += tu * Complex(Va - dc_mu_a + ja, cja);
+            v -= tv * Complex(Vb - dc_mu_b + jb, -1.0 * cjb);
+            u += tv * D;
+            v += tu * std::conj(D);
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+            u += tu * na;
+            v -= tv * nb;
+#endif
+#ifdef CURRENT_CORRECTIONS
+            {
+                std::vector<Complex> *dd[3] = {&ddx, &ddy, &ddz};
+                for (int d = 0; d < CODEDIM; d++) {
+                    u += U(*dd[d], n)[i] * ga[d];
+                    v -= V(*dd[d], n)[i] * gb[d];
+                }
+            }
+#endif
+            u += lu * aa;
+            v -= lv * ab;
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+            u += U(dalap, n)[i] * (-0.25);
+            v -= V(dalap, n)[i] * (-0.25);
+#endif
+#endif
+            out[(size_t)n * N + i] = u;
+            out[(size_t)S * N + (size_t)n * N + i] = v;
+        }
+    }
+    /* quasiparticle energies and subtraction (pca_kernels.cu:806-833) */
+#pragma omp parallel for
+    for (int n = 0; n < S; n++) {
+        double e = 0.0;
+        for (int i = 0; i < N; i++) {
+            Complex p = std::conj(U(w, n)[i]) * out[(size_t)n * N + i] +
+                        std::conj(V(w, n)[i]) * out[(size_t)S * N + (size_t)n * N + i];
+            e += p.real() * WTD_DV;
+        }
+        qpe[n] = e;
+        for (int i = 0; i < N; i++) {
+            out[(size_t)n * N + i] -= U(w, n)[i] * e;
+            out[(size_t)S * N + (size_t)n * N + i] -= V(w, n)[i] * e;
+        }
+    }
+}
+
+/* densities -> potentials block shared by both half steps (pca.c:1424-1457) */
+static void half_step_densities(int it_next, int grads)
+{
+    derivatives(y, grads);
+    calculate_densities(y, grads);
+    if (grads) density_tau();
+    compute_potentials(it_next);
+    alpha_laplace(y);
+}
+
+static int scheme_slots() { return NHIST; }
+
+} // namespace orc
+
+using namespace orc;
+
+extern "C" {
+
+int orc_numel(void) { return N; }
+int orc_codedim(void) { return CODEDIM; }
+int orc_nhist(void) { return NHIST; }
+int orc_dims(int *d) { d[0] = AXN[0]; d[1] = AXN[1]; d[2] = AXN[2]; return 0; }
+int orc_functional(void) { return FUNCTIONAL; }
+int orc_const_mass(void)
+{
+#ifdef FAST_CONST_EFFECTIVE_MASS_MODE
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+/* constants (memcopy_const / memcopy_const_params / memcopy_const_sclgth / memcopy_extra_data;
+ * wslda_cuda_utils.h:47-105) */
+int orc_set_constants(double mu_a, double mu_b, double ec, double t0, double dt, double kF, double sclgth)
+{
+    dc_mu_a = mu_a; dc_mu_b = mu_b; dc_ec = ec; dc_t0 = t0; dc_dt = dt; dc_kF = kF;
+    dc_eF = kF * kF / 2.; dc_nF = kF * kF * kF / (3. * M_PI * M_PI); dc_sclgth = sclgth;
+    md.sclgth = sclgth; md.dt = dt; md.ec = ec;
+    return 0;
+}
+int orc_set_params(const double *p)
+{
+    for (int k = 0; k < MAX_USER_PARAMS; k++) { dc_params[k] = p[k]; md.params[k] = p[k]; }
+    return 0;
+}
+int orc_set_extra_data(const void *d, size_t size)
+{
+    extra.assign((const unsigned char *)d, (const unsigned char *)d + size);
+    dc_extra_data = size ? extra.data() : nullptr;
+    dc_extra_data_size = size;
+    return 0;
+}
+
+/* states: y = [u_0..u_{S-1}, v_0..v_{S-1}] as interleaved (re, im) doubles; pots: 12N */
+int orc_setup(int nwf, const double *yin, const double *potsin, const double *fbeta,
+              const double *kyin, const double *kzin, const int *cntin, int it0)
+{
+    S = nwf;
+    for (int d = 0; d < 3; d++) make_plan(plans[d], AXN[d]);
+    size_t M = (size_t)2 * S * N;
+    y.assign((const Complex *)yin, (const Complex *)yin + M);
+    for (int h = 0; h < 5; h++) fk[h].assign(h < NHIST ? M : 0, Complex(0.0, 0.0));
+    ddx.assign(M, Complex(0, 0));
+    ddy.assign(CODEDIM >= 2 ? M : 0, Complex(0, 0));
+    ddz.assign(CODEDIM >= 3 ? M : 0, Complex(0, 0));
+    dlap.assign(M, Complex(0, 0));
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+    dalap.assign(M, Complex(0, 0));
+#endif
+    dens.assign((size_t)12 * N, 0.0);
+    pots.assign(potsin, potsin + (size_t)12 * N);
+    fb.assign(fbeta, fbeta + S);
+    kky.assign(S, 0.0); kkz.assign(S, 0.0); cnt.assign(S, 1);
+    if (kyin) kky.assign(kyin, kyin + S);
+    if (kzin) kkz.assign(kzin, kzin + S);
+    if (cntin) cnt.assign(cntin, cntin + S);
+    qpe.assign(S, 0.0);
+    it_global = it0;
+    return 0;
+}
+
+/* initial measurement (pca.c:939-958): normalise, derivatives, all densities, tau */
+int orc_initial_measurement(void)
+{
+    normalize(y);
+    derivatives(y, 1);
+    calculate_densities(y, 1);
+    density_tau();
+    last_gradients = 1;
+    return 0;
+}
+
+/* nsteps ABM steps as one measurement block (pca.c:1401-1571); gradients are formed on the
+ * last step (const mass) or on every step (variable mass). */
+int orc_steps(int nsteps)
+{
+    Complex *f[5];
+    for (int h = 0; h < 5; h++) f[h] = fk[h].empty() ? nullptr : fk[h].data();
+    for (int s = 0; s < nsteps; s++) {
+        int last = (s == nsteps - 1);
+        int it = it_global;
+        /* predictor */
+        abm_step1(y.data(), f[0], f[1], f[2], f[3], f[4]);
+        normalize(y);
+        int grads = orc_const_mass() ? 0 : 1;
+        half_step_densities(it + 1, grads);
+        apply_hamiltonian(it + 1, y, dlap.data());
+        /* corrector */
+        abm_step4(dlap.data(), y.data(), f[NHIST - 1]);
+        normalize(y);
+        grads = orc_const_mass() ? (last ? 1 : 0) : 1;
+        half_step_densities(it + 1, grads);
+        last_gradients = grads;
+        Complex *tmp = f[NHIST - 1];
+        for (int h = NHIST - 1; h > 0; h--) f[h] = f[h - 1];
+        f[0] = tmp;
+        apply_hamiltonian(it + 1, y, f[0]);
+        it_global++;
+    }
+    /* keep the rotated order visible to getters */
+    std::vector<std::vector<Complex>> nv(5);
+    for (int h = 0; h < NHIST; h++) nv[h].assign(f[h], f[h] + (size_t)2 * S * N);
+    for (int h = 0; h < NHIST; h++) fk[h].swap(nv[h]);
+    return 0;
+}
+
+/* compute_energy (tdwslda_energy_generic.h:21-111 and the functional energy kernels) */
+int orc_energy(double *E)
+{
+    using namespace oedf;
+    int it = it_global;
+    wslda_density Dn = dens_view(dens.data());
+    wslda_potential P = pots_view(pots.data());
+    std::vector<double> e(11 * (size_t)N, 0.0);
+    const double VOL = WTD_VOLEL;
+    for (int i = 0; i < N; i++) {
+        int ix, iy, iz; decode(i, ix, iy, iz);
+        double na = Dn.rho_a[i], nb = Dn.rho_b[i];
+        double x1 = Dn.j_a_x[i], x2 = Dn.j_b_x[i];
+        double y1 = (CODEDIM >= 2) ? Dn.j_a_y[i] : 0.0, y2 = (CODEDIM >= 2) ? Dn.j_b_y[i] : 0.0;
+        double z1 = (CODEDIM >= 3) ? Dn.j_a_z[i] : 0.0, z2 = (CODEDIM >= 3) ? Dn.j_b_z[i] : 0.0;
+#if FUNCTIONAL == CUSTOMEDF
+        blockIdx.x = 0; blockDim.x = 1; threadIdx.x = i;
+        tdwslda_compute_energy(it, Dn, P, &e[EKIN * (size_t)N], &e[EPOT * (size_t)N], &e[EPAIR * (size_t)N], &e[ECURRENT * (size_t)N]);
+#else
+        double taua = Dn.tau_a[i], taub = Dn.tau_b[i];
+        taua -= p_reg(na) * (x1 * x1 + y1 * y1 + z1 * z1) / na;
+        taub -= p_reg(nb) * (x2 * x2 + y2 * y2 + z2 * z2) / nb;
+#if FUNCTIONAL == BDG
+        e[EKIN * (size_t)N + i] = 0.5 * (P.alpha_a[i] * taua + P.alpha_b[i] * taub) * VOL;
+        e[EPOT * (size_t)N + i] = 0.0;
+#else
+        double p = pol(na, nb);
+        e[EKIN * (size_t)N + i] = 0.5 * (alpha(p) * taua + alpha(-p) * taub) * VOL;
+        e[EPOT * (size_t)N + i] = funD(na, nb) * VOL;
+#endif
+        e[EPAIR * (size_t)N + i] = (P.delta[i] * std::conj(Dn.nu[i])).real() * (-1.0) * VOL;
+        e[ECURRENT * (size_t)N + i] = p_reg(na) * (x1 * x1 + y1 * y1 + z1 * z1) / (2. * na) * VOL +
+                                      p_reg(nb) * (x2 * x2 + y2 * y2 + z2 * z2) / (2. * nb) * VOL;
+#endif
+#ifdef ENABLE_V_EXT
+        e[EPOTEXT * (size_t)N + i] = (na * ORC_U_EXT(ix, iy, iz, it, SPINA) + nb * ORC_U_EXT(ix, iy, iz, it, SPINB)) * VOL;
+#endif
+#ifdef ENABLE_DELTA_EXT
+        e[EPAIREXT * (size_t)N + i] = (std::conj(Dn.nu[i]) * ORC_D_EXT(ix, iy, iz, it, P.delta[i])).real() * (-2.0) * VOL;
+#endif
+        e[NPARTA * (size_t)N + i] = na;
+        e[NPARTB * (size_t)N + i] = nb;
+#if CODEDIM >= 2
+        double xx = (double)(ix - NX / 2) * DX, yy = (double)(iy - NY / 2) * DY;
+        e[LZA * (size_t)N + i] = (xx * y1 - yy * x1) * VOL;
+        e[LZB * (size_t)N + i] = (xx * y2 - yy * x2) * VOL;
+#endif
+    }
+#ifdef ENABLE_MODIFY_ENERGIES
+    blockIdx.x = 0; blockDim.x = 1;
+    for (int i = 0; i < N; i++) { threadIdx.x = i; modify_energies(it, Dn, P, e.data()); }
+#endif
+    for (int k = 0; k < TDWSLDAITEMS; k++) {
+        double s = 0.0;
+        for (int i = 0; i < N; i++) s += e[(size_t)k * N + i];
+        E[k] = s;
+    }
+    E[NPARTA] *= VOL;
+    E[NPARTB] *= VOL;
+    return 0;
+}
+
+int orc_get_states(double *out) { std::memcpy(out, y.data(), y.size() * sizeof(Complex)); return 0; }
+int orc_get_densities(double *out) { std::memcpy(out, dens.data(), dens.size() * sizeof(double)); return 0; }
+int orc_get_potentials(double *out) { std::memcpy(out, pots.data(), pots.size() * sizeof(double)); return 0; }
+int orc_get_qpe(double *out) { std::memcpy(out, qpe.data(), qpe.size() * sizeof(double)); return 0; }
+int orc_get_history(int slot, double *out)
+{
+    if (slot < 0 || slot >= NHIST) return -1;
+    std::memcpy(out, fk[slot].data(), fk[slot].size() * sizeof(Complex));
+    return 0;
+}
+int orc_get_it(void) { return it_global; }
+int orc_set_threads(int n)
+{
+#ifdef _OPENMP
+    omp_set_num_threads(n);
+#endif
+    return n;
+}
+
+/* standalone transform of one lattice field, for checking the FFT against numpy */
+int orc_fft_field(double *data, int sign)
+{
+    for (int d = 0; d < 3; d++) if (plans[d].n != AXN[d]) make_plan(plans[d], AXN[d]);
+    fftn((Complex *)data, sign);
+    return 0;
+}
+/* spectral derivatives of one complex field: outputs dx, dy, dz, lap (N complex each) */
+int orc_derivatives_field(const double *f, double *dx, double *dy, double *dz, double *lap)
+{
+    for (int d = 0; d < 3; d++) if (plans[d].n != AXN[d]) make_plan(plans[d], AXN[d]);
+    derivs_one((const Complex *)f, (Complex *)dx, CODEDIM >= 2 ? (Complex *)dy : nullptr,
+               CODEDIM >= 3 ? (Complex *)dz : nullptr, (Complex *)lap);
+    return 0;
+}
+}

@@ -1,0 +1,115 @@
+"""Generate golden vectors from the REFERENCE's own CUDA kernels (run on a B200).
+
+Loads oracle/_ref/<project>/libref.so (hpc-engine/*.cu compiled unmodified for sm_100a plus
+oracle/ref_harness.cu, built in the build container by `make -C oracle ref PROJECT=<p>`),
+regenerates the seeded inputs of wslda_b200.projects, runs the reference's time loop and
+saves the outputs as tests/golden/<project>.npz.  The fixtures pin the CPU oracle
+(tests/test_oracle_golden.py) and the CUDA library (tests/test_gpu_parity.py).
+
+    python tests/golden/make_golden.py --out gpurun_out/golden [project ...]
+"""
+import argparse
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+from wslda_b200 import projects as P  # noqa: E402
+
+# (project, nwf, steps per measurement, measurements, store full states?)
+CASES = {
+    "t1d_custom": (24, 3, 2, True),
+    "t1d_aslda": (24, 3, 2, True),
+    "t2d_slda": (24, 3, 2, True),
+    "t2d_bdg": (24, 3, 2, True),
+    "t3d_slda": (24, 3, 2, True),
+    "t3d_aslda": (24, 3, 2, True),
+    "c1_bdg1d": (256, 100, 1, False),
+    "c2_slda2d": (16, 4, 1, False),
+    "c3_aslda3d": (8, 2, 1, False),
+    "c4_bdg2d": (16, 4, 1, False),
+    "c5_slda3d": (4, 2, 1, False),
+}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def case_inputs(name, nwf):
+    proj = P.Project(name)
+    seed = P.config_seed(name)
+    y0 = P.make_states(proj, nwf, seed)
+    occ = P.make_occupations(nwf)
+    pots = P.make_potentials(proj)
+    params = P.stirrer_params(proj, seed) if proj.cfg.get("stirrer_params") else proj.params
+    extra = P.make_extra(proj, seed)
+    return proj, y0, occ, pots, params, extra
+
+
+def state_moments(y, nwf, n):
+    """Per-state checksums: norm of u, norm of v, sum of u weighted by a fixed ramp."""
+    a = y.reshape(2, nwf, n)
+    ramp = np.linspace(-1.0, 1.0, n)
+    return np.stack([np.sum(np.abs(a[0]) ** 2, 1), np.sum(np.abs(a[1]) ** 2, 1),
+                     (a[0] @ ramp).real, (a[0] @ ramp).imag, (a[1] @ ramp).real, (a[1] @ ramp).imag], 1)
+
+
+def run_case(name, out_dir):
+    nwf, nsteps, nmeas, full = CASES[name]
+    proj, y0, occ, pots, params, extra = case_inputs(name, nwf)
+    so = os.path.join(REPO, "oracle", "_ref", name, "libref.so")
+    lib = ctypes.CDLL(so, mode=ctypes.RTLD_LOCAL)
+    lib.refh_numel.restype = ctypes.c_int
+    lib.refh_nhist.restype = ctypes.c_int
+    n = lib.refh_numel()
+    nh = lib.refh_nhist()
+    assert n == proj.numel
+    c = proj.constants()
+    lib.refh_run.argtypes = ([ctypes.c_int] + [_dp] * 5 + [ctypes.POINTER(ctypes.c_int)] + [ctypes.c_double] * 7 +
+                             [_dp, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_dp] * 7)
+    M = 2 * nwf * n
+    y = np.zeros(M, dtype=np.complex128)
+    dens = np.zeros(12 * n)
+    potso = np.zeros(12 * n)
+    en = np.zeros(11)
+    qpe = np.zeros(nwf)
+    hist = np.zeros(nh * M, dtype=np.complex128)
+    ms = np.zeros(1)
+    ex = np.ascontiguousarray(extra)
+    rc = lib.refh_run(nwf, _p(y0.view(np.float64)), _p(pots), _p(occ), None, None, None,
+                      c["mu_a"], c["mu_b"], c["ec"], c["t0"], c["dt"], c["kF"], c["sclgth"],
+                      _p(np.ascontiguousarray(params)), ex.ctypes.data if ex.size else None, ex.nbytes,
+                      nsteps, nmeas, 0, _p(y.view(np.float64)), _p(dens), _p(potso), _p(en), _p(qpe),
+                      _p(hist.view(np.float64)), _p(ms))
+    if rc != 0:
+        raise RuntimeError(f"{name}: refh_run returned {rc}")
+    rec = dict(nwf=nwf, nsteps=nsteps, nmeas=nmeas, densities=dens, potentials=potso, energy=en, qpe=qpe,
+               input_moments=state_moments(y0, nwf, n), moments=state_moments(y, nwf, n), ms_per_step=ms[0])
+    if full:
+        rec["states"] = y
+        rec["history0"] = hist[:M]
+    path = os.path.join(out_dir, f"{name}.npz")
+    np.savez_compressed(path, **rec)
+    print(f"{name}: nwf={nwf} steps={nsteps}x{nmeas} E={en[:7].sum():.12g} N={en[7]:.12g},{en[8]:.12g} "
+          f"ms/step={ms[0]:.3f} -> {path}")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=HERE)
+    ap.add_argument("projects", nargs="*")
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    for name in (a.projects or list(CASES)):
+        run_case(name, a.out)
+
+
+if __name__ == "__main__":
+    main()

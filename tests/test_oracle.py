@@ -1,0 +1,60 @@
+"""The CPU oracle's own arithmetic: FFT against numpy, spectral derivatives against analytic
+Gaussians (the known-answer tests of lib/wderiv/c/test-wderiv.c:91-111), conservation of the
+state norm and the ABM/normalisation structure of a step."""
+import numpy as np
+import pytest
+
+from oracle_lib import Oracle
+from parity_util import inputs
+
+SMALL = ["t1d_custom", "t1d_aslda", "t2d_slda", "t2d_bdg", "t3d_slda", "t3d_aslda"]
+
+
+@pytest.mark.parametrize("name", SMALL + ["c1_bdg1d", "c2_slda2d", "c4_bdg2d"])
+def test_fft_matches_numpy(name):
+    o = Oracle(name)
+    p = o.proj
+    rng = np.random.default_rng(1)
+    f = rng.standard_normal(p.numel) + 1j * rng.standard_normal(p.numel)
+    shape = p.dims[: p.codedim]
+    fw = o.fft_field(f, -1)
+    ref = np.fft.fftn(f.reshape(shape)).reshape(-1)
+    assert np.abs(fw - ref).max() / np.abs(ref).max() < 1e-14
+    bw = o.fft_field(fw, +1)
+    assert np.abs(bw / p.numel - f).max() < 1e-14
+
+
+@pytest.mark.parametrize("name", ["c1_bdg1d", "c2_slda2d", "c4_bdg2d"])
+def test_spectral_derivatives_of_gaussian(name):
+    """d/dx_d and laplacian of a periodic-enough Gaussian against the analytic result."""
+    o = Oracle(name)
+    p = o.proj
+    axes = [(np.arange(n) - n // 2) * d for n, d in zip(p.dims, (p.dx, p.dy, p.dz))][: p.codedim]
+    grids = np.meshgrid(*axes, indexing="ij")
+    width = min(p.dims[: p.codedim]) / 16.0 * max(p.dx, 1.0)
+    r2 = sum(g * g for g in grids)
+    f = np.exp(-r2 / (2 * width ** 2)) * (1 + 0.5j)
+    dx, dy, dz, lap = o.derivatives_field(f.reshape(-1))
+    ex_dx = (-grids[0] / width ** 2 * f).reshape(-1)
+    ex_lap = ((r2 / width ** 4 - p.codedim / width ** 2) * f).reshape(-1)
+    assert np.abs(dx - ex_dx).max() < 5e-6 * np.abs(ex_dx).max() + 1e-9
+    assert np.abs(lap - ex_lap).max() < 5e-5 * np.abs(ex_lap).max() + 1e-9
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_step_keeps_states_normalised(name):
+    proj, d = inputs(name, 16)
+    o = Oracle(name)
+    o.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+    o.initial_measurement()
+    o.steps(3)
+    y = o.states().reshape(2, 16, proj.numel)
+    norms = (np.abs(y[0]) ** 2 + np.abs(y[1]) ** 2).sum(1) * proj.dv
+    assert np.allclose(norms, 1.0, atol=1e-13)
+    e = o.energy()
+    assert np.all(np.isfinite(e))
+    dens = o.densities()
+    n = proj.numel
+    # particle number: sum of rho over the lattice, times dV, equals the energy slots 7, 8
+    assert abs(dens[2 * n:3 * n].sum() * {1: proj.dx, 2: proj.dx * proj.dy, 3: proj.dv}[proj.codedim] - e[7]) < 1e-10 * max(1, abs(e[7]))
+    assert o.lib.orc_get_it() == 3

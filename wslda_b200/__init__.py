@@ -1,0 +1,186 @@
+"""B200-native TD-(A)SLDA/BdG step for W-SLDA projects.
+
+The product is the per-project CUDA library ``libwtd.so`` (C ABI in ``include/wtd.h``).  This
+package builds it (``wslda_b200.build``) and mirrors the reference's host driver calls in
+Python for tests and benchmarks (:class:`TDRun`).  There is no CPU fallback: a context can
+only be created where the CUDA library loads and a GPU is present.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+from .projects import Project
+
+__all__ = ["Project", "TDRun", "load_library", "FP64", "MIXED_H64", "MIXED_H32"]
+
+FP64, MIXED_H64, MIXED_H32 = 0, 1, 2
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_LIBS = {}
+
+# every symbol include/wtd.h declares, with its ctypes signature
+SIGNATURES = {
+    "wtd_info": (ctypes.c_int, [_ip, _ip, _ip, _ip, _ip, _ip]),
+    "wtd_device_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
+    "wtd_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "wtd_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "wtd_error_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "wtd_set_constants": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_double] * 6),
+    "wtd_set_params": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "wtd_set_sclgth": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "wtd_set_extra_data": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    "wtd_process_params": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp]),
+    "wtd_upload_states": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "wtd_upload_potentials": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "wtd_upload_occupations": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _ip]),
+    "wtd_upload_history": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
+    "wtd_download_history": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
+    "wtd_initial_measurement": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "wtd_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "wtd_energy": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "wtd_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "wtd_time_index": (ctypes.c_int, [ctypes.c_void_p]),
+    "wtd_download_states": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "wtd_download_densities": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "wtd_download_potentials": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "wtd_download_qpe": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "wtd_device_pointers": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_dp), ctypes.POINTER(_dp)]),
+    "wtd_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "wtd_launch_count": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "wtd_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "wtd_pass_times": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _ip, _ip]),
+}
+
+
+def load_library(project, build=True):
+    """Load (building if needed) the CUDA library of a project."""
+    if project in _LIBS:
+        return _LIBS[project]
+    path = _build.lib_path(project)
+    if build:
+        path = _build.build(project)
+    if not os.path.exists(path):
+        raise RuntimeError(f"CUDA library for {project} not built ({path}); run python -m wslda_b200.build {project}")
+    lib = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIBS[project] = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+class WtdError(RuntimeError):
+    pass
+
+
+class TDRun:
+    """One TD run on one GPU: the reference driver's sequence (pca.c:749-1571) over the C ABI."""
+
+    def __init__(self, project, nwf, precision=FP64, device=0, build=True):
+        self.proj = project if isinstance(project, Project) else Project(project)
+        self.lib = load_library(self.proj.name, build=build)
+        self.nwf = int(nwf)
+        self.N = self.proj.numel
+        h = ctypes.c_void_p()
+        self._check(self.lib.wtd_create(ctypes.byref(h), self.nwf, int(precision), int(device)))
+        self.h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise WtdError(f"{self.proj.name}: {self.lib.wtd_error_string(rc).decode()} ({rc})")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.wtd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def setup(self, states, pots, occ, params, extra=None, const=None, it0=0, kky=None, kkz=None, cnt=None):
+        c = const or self.proj.constants()
+        self._check(self.lib.wtd_set_constants(self.h, c["mu_a"], c["mu_b"], c["ec"], c["t0"], c["dt"], c["kF"]))
+        self._check(self.lib.wtd_set_sclgth(self.h, c["sclgth"]))
+        self._params = np.ascontiguousarray(params, dtype=np.float64)
+        self._check(self.lib.wtd_set_params(self.h, _p(self._params)))
+        ex = np.ascontiguousarray(extra if extra is not None else np.zeros(0), dtype=np.float64)
+        self._check(self.lib.wtd_set_extra_data(self.h, ex.ctypes.data if ex.size else None, ex.nbytes))
+        self.upload_states(states)
+        self._check(self.lib.wtd_upload_potentials(self.h, _p(np.ascontiguousarray(pots, dtype=np.float64))))
+        cnt_p = None if cnt is None else np.ascontiguousarray(cnt, dtype=np.int32).ctypes.data_as(_ip)
+        kky = None if kky is None else np.ascontiguousarray(kky, dtype=np.float64)
+        kkz = None if kkz is None else np.ascontiguousarray(kkz, dtype=np.float64)
+        self._check(self.lib.wtd_upload_occupations(self.h, _p(np.ascontiguousarray(occ, dtype=np.float64)),
+                                                     _p(kky), _p(kkz), cnt_p))
+        self.it0 = it0
+
+    def upload_states(self, states):
+        st = np.ascontiguousarray(states, dtype=np.complex128)
+        self._check(self.lib.wtd_upload_states(self.h, _p(st.view(np.float64))))
+
+    def initial_measurement(self, it0=None):
+        self._check(self.lib.wtd_initial_measurement(self.h, int(self.it0 if it0 is None else it0)))
+
+    def steps(self, n):
+        self._check(self.lib.wtd_steps(self.h, int(n)))
+
+    def sync(self):
+        self._check(self.lib.wtd_sync(self.h))
+
+    def energy(self):
+        e = np.zeros(11)
+        self._check(self.lib.wtd_energy(self.h, _p(e)))
+        return e
+
+    def states(self, out=None):
+        a = out if out is not None else np.zeros(2 * self.nwf * self.N, dtype=np.complex128)
+        self._check(self.lib.wtd_download_states(self.h, _p(a.view(np.float64))))
+        return a
+
+    def densities(self, out=None):
+        a = out if out is not None else np.zeros(12 * self.N)
+        self._check(self.lib.wtd_download_densities(self.h, _p(a)))
+        return a
+
+    def potentials(self):
+        a = np.zeros(12 * self.N)
+        self._check(self.lib.wtd_download_potentials(self.h, _p(a)))
+        return a
+
+    def qpe(self):
+        a = np.zeros(self.nwf)
+        self._check(self.lib.wtd_download_qpe(self.h, _p(a)))
+        return a
+
+    def history(self, slot):
+        a = np.zeros(2 * self.nwf * self.N, dtype=np.complex128)
+        self._check(self.lib.wtd_download_history(self.h, int(slot), _p(a.view(np.float64))))
+        return a
+
+    def time_index(self):
+        return self.lib.wtd_time_index(self.h)
+
+    def launches(self):
+        return self.lib.wtd_launch_count(self.h)
+
+    def stream(self):
+        return self.lib.wtd_stream(self.h)
+
+    def set_timing(self, on=True):
+        self._check(self.lib.wtd_set_timing(self.h, 1 if on else 0))
+
+    def pass_times(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        na, nb = ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.wtd_pass_times(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(na), ctypes.byref(nb)))
+        return a.value, b.value, na.value, nb.value

@@ -1,0 +1,208 @@
+/*
+ * Compile-time configuration of a project: derives the evolution mode from the user's
+ * predefines.h exactly as hpc-engine/pca_settings.h:36-95,143-241 does, and defines the
+ * names user hook code relies on (NXYZ, DXYZ, LX, SPINA, XAXIS, energy slots, ...).
+ *
+ * Names and numeric values are kept identical to the reference because they are part of the
+ * plugin surface: problem-definition.h files written for W-SLDA test them (FUNCTIONAL==SLDA,
+ * CODEDIM, SPINA, ...) and the functional constants (A0..A2, G0, G1, GAMMA0, regularisation)
+ * are the published parameters of the SLDA/ASLDA energy density functional.
+ *
+ * Include after predefines.h.  CODEDIM (1, 2 or 3) is given on the compiler command line.
+ */
+#ifndef WTD_SETTINGS_H
+#define WTD_SETTINGS_H
+
+#ifndef CODEDIM
+#error "CODEDIM must be defined (1, 2 or 3)"
+#endif
+
+/* functional selectors (pca_settings.h:69-73) */
+#define SLDA 111
+#define ASLDA 112
+#define BDG 113
+#define CUSTOMEDF 114
+#define SLDAE 115
+
+/* integration schemes (pca_settings.h:203-205) */
+#define AB3AM4 34
+#define AB4AM5 45
+#define AB5AM5 55
+#ifndef INTEGRATION_SCHEME
+#define INTEGRATION_SCHEME AB4AM5
+#endif
+
+/* regularisation schemes (pca_settings.h:224-225) */
+#define SPHERICAL_CUTOFF 88
+#define CUBIC_CUTOFF 89
+
+/* self-consistent local solve of U and Delta (pca_settings.h:36-38) */
+#define UD_SCITERS 15
+#define UD_MIX_COEFF 0.75
+
+/* legacy spellings (pca_settings.h:52-63) */
+#ifdef SLDAE_FORCE_A1
+#define SLDA_FORCE_A1
+#endif
+#ifdef ASLDA_STABILIZATION_RETAIN_ABOVE_DENSITY
+#define SLDA_STABILIZATION_RETAIN_ABOVE_DENSITY ASLDA_STABILIZATION_RETAIN_ABOVE_DENSITY
+#endif
+#ifdef ASLDA_STABILIZATION_EXCLUDE_BELOW_DENISTY
+#define SLDA_STABILIZATION_EXCLUDE_BELOW_DENISTY ASLDA_STABILIZATION_EXCLUDE_BELOW_DENISTY
+#endif
+
+#if FUNCTIONAL==SLDAE
+#error "FUNCTIONAL SLDAE is not provided by this library (see DESIGN.md, scope)"
+#endif
+
+/* mode derivation (pca_settings.h:75-95, 186-222) */
+#if FUNCTIONAL==BDG
+#define BDG_MODE
+#define SLDA_FORCE_A1
+#endif
+#if FUNCTIONAL==SLDA
+#define SLDA_FORCE_A1
+#endif
+
+#ifdef SLDA_FORCE_A1
+#define A0 1.000
+#define A1 0.0
+#define A2 0.0
+#define FAST_CONST_EFFECTIVE_MASS_MODE
+#else
+#define A0 1.094
+#define A1 0.156
+#define A2 -0.532
+#define CURRENT_CORRECTIONS
+#endif
+
+#define G0 0.357
+#define G1 0.642
+
+#ifdef SLDA_STABILIZATION_EXCLUDE_BELOW_DENISTY
+#define P_NMIN SLDA_STABILIZATION_EXCLUDE_BELOW_DENISTY
+#else
+#define P_NMIN 1.0e-7
+#endif
+#ifdef SLDA_STABILIZATION_RETAIN_ABOVE_DENSITY
+#define P_NMAX SLDA_STABILIZATION_RETAIN_ABOVE_DENSITY
+#else
+#define P_NMAX 1.0e-5
+#endif
+#define P_ALPHA 1.0
+
+#ifdef ENABLE_MODIFY_POTENTIALS
+#undef BDG_MODE
+#endif
+#ifdef SLDA_FORCE_A1
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+#define FAST_CONST_EFFECTIVE_MASS_MODE
+#endif
+#endif
+#ifdef FAST_CONST_EFFECTIVE_MASS_MODE
+#undef CURRENT_CORRECTIONS
+#endif
+#ifdef BDG_MODE
+#undef CURRENT_CORRECTIONS
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+#define FAST_CONST_EFFECTIVE_MASS_MODE
+#endif
+#endif
+#ifdef ENABLE_VELOCITY_EXT
+#error "ENABLE_VELOCITY_EXT is not provided by this library (see DESIGN.md, scope)"
+#endif
+#ifdef SPINSYMMETRY_MODE
+#error "SPINSYMMETRY_MODE is not provided by this library (see DESIGN.md, scope)"
+#endif
+
+#if REGULARIZATION_SCHEME==CUBIC_CUTOFF
+#define USE_CUBIC_CUTOFF
+#define GAMMA0 -11.11
+#define REG_COEFF_K 2.442749607806335
+#define REG_COEFF_R0 (REG_COEFF_K/(4.0*M_PI*M_PI))
+#define REG_COEFF_R1 0.31786000
+#else
+#define GAMMA0 -11.11
+#define REG_COEFF_R0 (1./(2.0*M_PI*M_PI))
+#define REG_COEFF_R1 0.5
+#endif
+
+#ifndef DENSEPSILON
+#define DENSEPSILON 1.0e-8
+#endif
+#ifndef MAX_USER_PARAMS
+#define MAX_USER_PARAMS 32
+#endif
+
+/* lattice helpers (pca_settings.h:123-139) */
+#define NUMERICAL_ZERO 1.0e-16
+#define DXYZ (DX*DY*DZ)
+#define DXY (DX*DY)
+#define LX (DX*NX)
+#define LY (DY*NY)
+#define LZ (DZ*NZ)
+#define LXYZ (LX*LY*LZ)
+#define NXYZ (NX*NY*NZ)
+#define NXY (NX*NY)
+#define LXY (LX*LY)
+
+#define SPINA 0
+#define SPINB 1
+#define XAXIS 0
+#define YAXIS 1
+#define ZAXIS 2
+
+/* observable slots written by compute_energy (pca_settings.h:143-158) */
+#define ENERGYITEMS 7
+#define EKIN 0
+#define EPOT 1
+#define EPAIR 2
+#define ECURRENT 3
+#define EPOTEXT 4
+#define EPAIREXT 5
+#define EVELEXT 6
+#define TDWSLDAITEMS (ENERGYITEMS+4)
+#define NPARTA 7
+#define NPARTB 8
+#define LZA 9
+#define LZB 10
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+#ifndef M_PI_2
+#define M_PI_2 1.570796326794896558
+#endif
+#ifndef API_VERSION
+#define API_VERSION 20220218
+#endif
+
+/* ---- derived per-dimension quantities used by this library ---- */
+#if CODEDIM==1
+#define WTD_NUMEL (NX)
+#define WTD_DV (DX)                 /* measure of one lattice point in norms and <psi|H|psi> */
+#define WTD_LPERP ((double)(LY*LZ)) /* plane-wave normalisation divided out of densities */
+#define WTD_VOLEL (DXYZ*NY*NZ)     /* VOLUME_ELEMENT of the energy kernels */
+#elif CODEDIM==2
+#define WTD_NUMEL (NX*NY)
+#define WTD_DV (DX*DY)
+#define WTD_LPERP ((double)(LZ))
+#define WTD_VOLEL (DXYZ*NZ)
+#else
+#define WTD_NUMEL (NX*NY*NZ)
+#define WTD_DV (DXYZ)
+#define WTD_LPERP (1.0)
+#define WTD_VOLEL (DXYZ)
+#endif
+
+#if INTEGRATION_SCHEME==AB3AM4
+#define WTD_NHIST 3
+#elif INTEGRATION_SCHEME==AB4AM5
+#define WTD_NHIST 4
+#elif INTEGRATION_SCHEME==AB5AM5
+#define WTD_NHIST 5
+#else
+#error "INTEGRATION_SCHEME must be AB3AM4, AB4AM5 or AB5AM5"
+#endif
+
+#endif /* WTD_SETTINGS_H */

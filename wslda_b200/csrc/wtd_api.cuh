@@ -1,0 +1,619 @@
+/*
+ * Host side of the fused C ABI (include/wtd.h): a context owns the device state of one run —
+ * states, the ABM history ring, densities, potentials, per-point H coefficients and the
+ * density partial slots — and orders all work on one CUDA stream.
+ *
+ * One step (wtd_steps) issues, on the context stream:
+ *   pass A  -> reduce density slots -> [tau] -> potentials(it+1) -> coefficients(it+1)
+ *   pass B  -> reduce density slots -> [tau] -> potentials(it+1) -> coefficients(it+1)
+ * which is the reference's per-step sequence (hpc-engine/pca.c:1401-1571) with its ~30
+ * whole-array kernels per half step folded into one stream pass.
+ */
+#ifndef WTD_API_CUH
+#define WTD_API_CUH
+
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include "wtd.h"
+#include "wtd_aux.cuh"
+
+#if CODEDIM == 1
+typedef Geo<NX, 1, 1> WG;
+#elif CODEDIM == 2
+typedef Geo<NX, NY, 1> WG;
+#else
+typedef Geo<NX, NY, NZ> WG;
+#endif
+
+#ifdef FAST_CONST_EFFECTIVE_MASS_MODE
+#define WTD_VAR false
+#else
+#define WTD_VAR true
+#endif
+
+struct wtd_ctx {
+    int dev, S, prec;
+    size_t ysz, hsz;            /* bytes per state array (y) and per history slot */
+    void *y;
+    void *hist[WTD_NHIST];      /* physical slots */
+    int head;                   /* ring position 0 = physical slot head */
+    double *cf, *occ, *kp2, *wcnt, *dslot, *qpe, *dens, *pots, *ework, *eout;
+    double2 *tw;
+    double *ktab;
+    double2 *stage;             /* FP64 staging for conversions (mixed precision) */
+    void *extra;
+    size_t extra_bytes;
+    int grid;
+    int it;
+    int fk_given;
+    int have_coef;
+    double dt;
+    cudaStream_t st;
+    long long launches;
+    /* optional device timing of the fused passes: events around each pass, summed on demand */
+    int timing;
+    cudaEvent_t ev[2][2][4096];
+    int nev[2];
+};
+
+static int wtd_cuerr(cudaError_t e) { return e == cudaSuccess ? WTD_OK : WTD_ERR_CUDA; }
+#define WTD_TRY(x) do { int _r = (x); if (_r) return _r; } while (0)
+#define WTD_CU(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return WTD_ERR_CUDA; } while (0)
+#define WTD_LAUNCHED(ctx) do { (ctx)->launches++; cudaError_t _e = cudaGetLastError(); if (_e != cudaSuccess) return WTD_ERR_CUDA; } while (0)
+
+static size_t elem_bytes_y(int prec) { return prec == WTD_FP64 ? sizeof(double2) : sizeof(float2); }
+static size_t elem_bytes_h(int prec) { return prec == WTD_MIXED_H32 ? sizeof(float2) : sizeof(double2); }
+
+/* ---------------------------------------------------------------------------------------
+ * fused pass dispatch
+ * -------------------------------------------------------------------------------------*/
+template <typename TC, int NBUF> static constexpr size_t fused_smem() { return FusedSmem<WG, TC, NBUF>::bytes; }
+static constexpr size_t WTD_SMEM_MAX = 232448;
+
+template <typename TY, typename TH, typename TC, int PASS, bool GRAD>
+static int launch_pass_t(wtd_ctx *c, StepArgs &a)
+{
+    constexpr int NBUF = WTD_VAR ? 4 : (GRAD ? 3 : 2);
+    constexpr size_t sm = fused_smem<TC, NBUF>();
+    if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+    else {
+        auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD>;
+        static bool attr = false;
+        if (!attr) {
+            WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            attr = true;
+        }
+        int threads = WG::ntot >= 512 ? 512 : ((WG::ntot + 31) / 32) * 32;
+        k<<<c->grid, threads, sm, c->st>>>(a, c->tw, c->ktab);
+        WTD_LAUNCHED(c);
+    }
+    return WTD_OK;
+}
+
+template <int PASS, bool GRAD>
+static int launch_pass(wtd_ctx *c, StepArgs &a)
+{
+    if (c->prec == WTD_FP64) return launch_pass_t<double2, double2, double, PASS, GRAD>(c, a);
+    if (c->prec == WTD_MIXED_H64) return launch_pass_t<float2, double2, float, PASS, GRAD>(c, a);
+    return launch_pass_t<float2, float2, float, PASS, GRAD>(c, a);
+}
+
+static void ring_slots(wtd_ctx *c, void **slot)
+{
+    for (int r = 0; r < WTD_NHIST; r++) slot[r] = c->hist[(c->head + r) % WTD_NHIST];
+}
+
+static StepArgs make_args(wtd_ctx *c)
+{
+    StepArgs a;
+    memset(&a, 0, sizeof(a));
+    a.y = c->y;
+    ring_slots(c, a.slot);
+    a.cf = c->cf; a.occ = c->occ; a.kp2 = c->kp2; a.wcnt = c->wcnt;
+    a.dslot = c->dslot; a.qpe = c->qpe; a.dt = c->dt; a.S = c->S;
+    a.fk_given = c->fk_given;
+    a.accumulate = 0;
+    return a;
+}
+
+static int run_pass(wtd_ctx *c, int pass, bool grad)
+{
+    StepArgs a = make_args(c);
+    if (c->timing && pass < 2 && c->nev[pass] < 4096) {
+        cudaEventRecord(c->ev[pass][0][c->nev[pass]], c->st);
+        int r = (pass == 0) ? (grad ? launch_pass<0, true>(c, a) : launch_pass<0, false>(c, a))
+                            : (grad ? launch_pass<1, true>(c, a) : launch_pass<1, false>(c, a));
+        cudaEventRecord(c->ev[pass][1][c->nev[pass]], c->st);
+        c->nev[pass]++;
+        return r;
+    }
+    if (pass == 0) return grad ? launch_pass<0, true>(c, a) : launch_pass<0, false>(c, a);
+    if (pass == 1) return grad ? launch_pass<1, true>(c, a) : launch_pass<1, false>(c, a);
+    return grad ? launch_pass<2, true>(c, a) : launch_pass<2, false>(c, a);
+}
+
+/* densities from the slots, tau, potentials and H coefficients at time index it */
+static int after_pass(wtd_ctx *c, bool full, int it)
+{
+    constexpr int N = WTD_NUMEL;
+    int nb = (12 * N + 255) / 256;
+    wtd_dens_reduce<<<nb, 256, 0, c->st>>>(c->dslot, c->grid, c->dens, N, full ? 1 : 0, 1.0 / WTD_LPERP);
+    WTD_LAUNCHED(c);
+    if (full) {
+        constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
+        if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+        static bool attr = false;
+        if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_tau_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+        wtd_tau_kernel<WG><<<2, 512, sm, c->st>>>(c->dens, c->tw, c->ktab);
+        WTD_LAUNCHED(c);
+    }
+    if (it < 0) return WTD_OK;
+    wslda_density D = convert_into_wslda_density(c->dens, N);
+    wslda_potential P = convert_into_wslda_potential(c->pots, N, NULL);
+    int pb = (N + 127) / 128;
+    wtd_potentials_kernel<<<pb, 128, 0, c->st>>>(it, D, P, 1.0);
+    WTD_LAUNCHED(c);
+#ifdef ENABLE_MODIFY_POTENTIALS
+    modify_potentials<<<pb, 128, 0, c->st>>>(it, D, P);
+    WTD_LAUNCHED(c);
+#endif
+    wtd_prep_coef<<<pb, 128, 0, c->st>>>(it, P, c->cf);
+    WTD_LAUNCHED(c);
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+    {
+        constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
+        if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+        static bool attr = false;
+        if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_prep_var<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+        wtd_prep_var<WG><<<2, 1024, sm, c->st>>>(c->cf, c->tw, c->ktab);
+        WTD_LAUNCHED(c);
+    }
+#endif
+    c->have_coef = 1;
+    return WTD_OK;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * C ABI
+ * -------------------------------------------------------------------------------------*/
+extern "C" {
+
+int wtd_info(int *dims, int *numel, int *codedim, int *nhist, int *functional, int *const_mass)
+{
+    if (dims) { dims[0] = WG::N0; dims[1] = WG::N1; dims[2] = WG::N2; }
+    if (numel) *numel = WTD_NUMEL;
+    if (codedim) *codedim = CODEDIM;
+    if (nhist) *nhist = WTD_NHIST;
+    if (functional) *functional = FUNCTIONAL;
+    if (const_mass) *const_mass = WTD_VAR ? 0 : 1;
+    return WTD_OK;
+}
+
+size_t wtd_device_bytes(int nwf, int precision)
+{
+    size_t n2 = (size_t)2 * nwf * WTD_NUMEL;
+    return n2 * (elem_bytes_y(precision) + WTD_NHIST * elem_bytes_h(precision)) +
+           (size_t)160 * 12 * WTD_NUMEL * sizeof(double);
+}
+
+const char *wtd_error_string(int code)
+{
+    switch (code) {
+    case WTD_OK: return "ok";
+    case WTD_ERR_ARG: return "invalid argument";
+    case WTD_ERR_CUDA: return "CUDA error";
+    case WTD_ERR_UNSUPPORTED: return "lattice/mode not supported by this build";
+    case WTD_ERR_STATE: return "call out of order";
+    case WTD_ERR_NOMEM: return "out of device memory";
+    default: return "unknown error";
+    }
+}
+
+int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
+{
+    if (!out || nwf <= 0 || precision < 0 || precision > 2) return WTD_ERR_ARG;
+    *out = NULL;
+    WTD_CU(cudaSetDevice(device));
+    wtd_ctx *c = (wtd_ctx *)calloc(1, sizeof(wtd_ctx));
+    if (!c) return WTD_ERR_NOMEM;
+    c->dev = device; c->S = nwf; c->prec = precision;
+    const size_t N = WTD_NUMEL, n2 = (size_t)2 * nwf * N;
+    c->ysz = n2 * elem_bytes_y(precision);
+    c->hsz = n2 * elem_bytes_h(precision);
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    /* one resident CTA per SM for the 2-D fused pass; more for tiny lattices */
+    int per_sm = 1;
+    {
+        size_t sm = (precision == WTD_FP64) ? fused_smem<double, WTD_VAR ? 4 : 3>() : fused_smem<float, WTD_VAR ? 4 : 3>();
+        per_sm = (int)(200000 / (sm + 1024));
+        int thr = WG::ntot >= 512 ? 512 : ((WG::ntot + 31) / 32) * 32;
+        int by_thr = 2048 / thr;
+        if (per_sm > by_thr) per_sm = by_thr;
+        if (per_sm > 8) per_sm = 8;
+        if (per_sm < 1) per_sm = 1;
+    }
+    c->grid = nsm * per_sm;
+    if (c->grid > nwf) c->grid = nwf;
+    cudaError_t e = cudaSuccess;
+#define ALLOC(p, bytes) if (e == cudaSuccess) e = cudaMalloc((void **)&(p), (bytes))
+    ALLOC(c->y, c->ysz);
+    for (int h = 0; h < WTD_NHIST; h++) ALLOC(c->hist[h], c->hsz);
+    ALLOC(c->cf, (size_t)CF_COUNT * N * sizeof(double));
+    ALLOC(c->occ, nwf * sizeof(double));
+    ALLOC(c->kp2, nwf * sizeof(double));
+    ALLOC(c->wcnt, nwf * sizeof(double));
+    ALLOC(c->dslot, (size_t)c->grid * 12 * N * sizeof(double));
+    ALLOC(c->qpe, nwf * sizeof(double));
+    ALLOC(c->dens, 12 * N * sizeof(double));
+    ALLOC(c->pots, 12 * N * sizeof(double));
+    ALLOC(c->ework, (size_t)TDWSLDAITEMS * N * sizeof(double));
+    ALLOC(c->eout, 16 * sizeof(double));
+    ALLOC(c->tw, WG::twtotal * sizeof(double2));
+    ALLOC(c->ktab, 6 * 128 * sizeof(double));
+    if (precision != WTD_FP64) ALLOC(c->stage, n2 * sizeof(double2));
+#undef ALLOC
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { wtd_destroy(c); return e == cudaErrorMemoryAllocation ? WTD_ERR_NOMEM : WTD_ERR_CUDA; }
+    cudaMemsetAsync(c->cf, 0, (size_t)CF_COUNT * N * sizeof(double), c->st);
+    cudaMemsetAsync(c->qpe, 0, nwf * sizeof(double), c->st);
+    cudaMemsetAsync(c->dens, 0, 12 * N * sizeof(double), c->st);
+    /* FFT twiddles e^{-2 pi i t/n} and wave-number tables of digit-reversed positions */
+    {
+        double2 tw[WG::twtotal];
+        double kt[6 * 128];
+        memset(kt, 0, sizeof(kt));
+        const double Lax[3] = {LX, LY, LZ};
+        for (int a = 0; a < 3; a++) {
+            int n = WG::n(a);
+            for (int t = 0; t < n; t++) {
+                long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)t / (long double)n;
+                tw[WG::twoff(a) + t] = make_double2((double)cosl(ang), -(double)sinl(ang));
+            }
+            for (int p = 0; p < n && p < 128; p++) {
+                int f = dif_freq(n, p);
+                double k = (f < n / 2) ? 2. * M_PI / Lax[a] * (double)f : 2. * M_PI / Lax[a] * (double)(f - n);
+                kt[a * 128 + p] = (n > 1) ? k : 0.0;
+                kt[(3 + a) * 128 + p] = (n > 1 && f != n / 2) ? k : 0.0;
+            }
+        }
+        cudaMemcpyAsync(c->tw, tw, sizeof(tw), cudaMemcpyHostToDevice, c->st);
+        cudaMemcpyAsync(c->ktab, kt, sizeof(kt), cudaMemcpyHostToDevice, c->st);
+    }
+    /* defaults: f_n = 0, no plane-wave momentum, unit degeneracy */
+    {
+        double *h = (double *)calloc(nwf, sizeof(double));
+        cudaMemcpy(c->occ, h, nwf * sizeof(double), cudaMemcpyHostToDevice);
+        cudaMemcpy(c->kp2, h, nwf * sizeof(double), cudaMemcpyHostToDevice);
+        for (int i = 0; i < nwf; i++) h[i] = 1.0;
+        cudaMemcpy(c->wcnt, h, nwf * sizeof(double), cudaMemcpyHostToDevice);
+        free(h);
+    }
+    for (int h = 0; h < WTD_NHIST; h++) cudaMemsetAsync(c->hist[h], 0, c->hsz, c->st);
+    c->fk_given = 1;
+    e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) { wtd_destroy(c); return WTD_ERR_CUDA; }
+    *out = c;
+    return WTD_OK;
+}
+
+int wtd_destroy(wtd_ctx *c)
+{
+    if (!c) return WTD_OK;
+    cudaSetDevice(c->dev);
+    if (c->st) cudaStreamSynchronize(c->st);
+    if (c->timing)
+        for (int p = 0; p < 2; p++)
+            for (int k = 0; k < 2; k++)
+                for (int i = 0; i < 4096; i++) cudaEventDestroy(c->ev[p][k][i]);
+    void *ptrs[] = {c->y, c->cf, c->occ, c->kp2, c->wcnt, c->dslot, c->qpe, c->dens, c->pots, c->ework,
+                    c->eout, c->tw, c->ktab, c->stage, c->extra};
+    for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) if (ptrs[i]) cudaFree(ptrs[i]);
+    for (int h = 0; h < WTD_NHIST; h++) if (c->hist[h]) cudaFree(c->hist[h]);
+    if (c->st) cudaStreamDestroy(c->st);
+    free(c);
+    return WTD_OK;
+}
+
+int wtd_set_constants(wtd_ctx *c, double mu_a, double mu_b, double ec, double t0, double dt, double kF)
+{
+    if (!c) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    double eF = kF * kF / 2., nF = kF * kF * kF / (3. * M_PI * M_PI);
+    WTD_CU(cudaMemcpyToSymbol(dc_mu_a, &mu_a, sizeof(double)));
+    WTD_CU(cudaMemcpyToSymbol(dc_mu_b, &mu_b, sizeof(double)));
+    WTD_CU(cudaMemcpyToSymbol(dc_ec, &ec, sizeof(double)));
+    WTD_CU(cudaMemcpyToSymbol(dc_t0, &t0, sizeof(double)));
+    WTD_CU(cudaMemcpyToSymbol(dc_dt, &dt, sizeof(double)));
+    WTD_CU(cudaMemcpyToSymbol(dc_kF, &kF, sizeof(double)));
+    WTD_CU(cudaMemcpyToSymbol(dc_eF, &eF, sizeof(double)));
+    WTD_CU(cudaMemcpyToSymbol(dc_nF, &nF, sizeof(double)));
+    hc_mu_a = mu_a; hc_mu_b = mu_b; hc_ec = ec; hc_t0 = t0; hc_dt = dt; hc_kF = kF; hc_eF = eF; hc_nF = nF;
+    md.dt = dt; md.ec = ec;
+    c->dt = dt;
+    return WTD_OK;
+}
+
+int wtd_set_params(wtd_ctx *c, const double *params)
+{
+    if (!c || !params) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    WTD_CU(cudaMemcpyToSymbol(dc_params, params, MAX_USER_PARAMS * sizeof(double)));
+    memcpy(md.params, params, MAX_USER_PARAMS * sizeof(double));
+    return WTD_OK;
+}
+
+int wtd_set_sclgth(wtd_ctx *c, double a)
+{
+    if (!c) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    WTD_CU(cudaMemcpyToSymbol(dc_sclgth, &a, sizeof(double)));
+    hc_sclgth = a;
+    md.sclgth = a;
+    return WTD_OK;
+}
+
+int wtd_set_extra_data(wtd_ctx *c, const void *host, size_t bytes)
+{
+    if (!c || (bytes && !host)) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    if (c->extra) { cudaFree(c->extra); c->extra = NULL; }
+    if (bytes) {
+        WTD_CU(cudaMalloc(&c->extra, bytes));
+        WTD_CU(cudaMemcpy(c->extra, host, bytes, cudaMemcpyHostToDevice));
+    }
+    c->extra_bytes = bytes;
+    WTD_CU(cudaMemcpyToSymbol(dc_extra_data, &c->extra, sizeof(void *)));
+    WTD_CU(cudaMemcpyToSymbol(dc_extra_data_size, &bytes, sizeof(size_t)));
+    return WTD_OK;
+}
+
+int wtd_process_params(wtd_ctx *c, double *params, double *kF, double *mu)
+{
+    if (!params || !kF || !mu) return WTD_ERR_ARG;
+    process_params(params, kF, mu, c ? c->extra_bytes : 0, NULL);
+    return WTD_OK;
+}
+
+static int upload_array(wtd_ctx *c, void *dst, int prec_elem64, const double *host)
+{
+    const size_t n2 = (size_t)2 * c->S * WTD_NUMEL;
+    if (prec_elem64) {
+        WTD_CU(cudaMemcpyAsync(dst, host, n2 * sizeof(double2), cudaMemcpyHostToDevice, c->st));
+    } else {
+        WTD_CU(cudaMemcpyAsync(c->stage, host, n2 * sizeof(double2), cudaMemcpyHostToDevice, c->st));
+        wtd_convert_in<float2><<<(unsigned)((n2 + 255) / 256), 256, 0, c->st>>>(c->stage, (float2 *)dst, n2);
+        WTD_LAUNCHED(c);
+    }
+    return WTD_OK;
+}
+static int download_array(wtd_ctx *c, const void *src, int prec_elem64, double *host)
+{
+    const size_t n2 = (size_t)2 * c->S * WTD_NUMEL;
+    if (prec_elem64) {
+        WTD_CU(cudaMemcpyAsync(host, src, n2 * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+    } else {
+        wtd_convert_out<float2><<<(unsigned)((n2 + 255) / 256), 256, 0, c->st>>>((const float2 *)src, c->stage, n2);
+        WTD_LAUNCHED(c);
+        WTD_CU(cudaMemcpyAsync(host, c->stage, n2 * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+    }
+    WTD_CU(cudaStreamSynchronize(c->st));
+    return WTD_OK;
+}
+
+int wtd_upload_states(wtd_ctx *c, const double *host)
+{
+    if (!c || !host) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    return upload_array(c, c->y, c->prec == WTD_FP64, host);
+}
+
+int wtd_download_states(wtd_ctx *c, double *host)
+{
+    if (!c || !host) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    return download_array(c, c->y, c->prec == WTD_FP64, host);
+}
+
+/* reference slot s (f_{s+1}, f1 newest) lives at ring position NH-1 for s = 0 (the "given"
+ * f_k) and at ring position s-1 for s >= 1 */
+static int ring_of_ref_slot(int s) { return s == 0 ? WTD_NHIST - 1 : s - 1; }
+
+int wtd_upload_history(wtd_ctx *c, int slot, const double *host)
+{
+    if (!c || !host || slot < 0 || slot >= WTD_NHIST) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    void *s[5];
+    ring_slots(c, s);
+    WTD_TRY(upload_array(c, s[ring_of_ref_slot(slot)], c->prec != WTD_MIXED_H32, host));
+    c->fk_given = 1;
+    return WTD_OK;
+}
+
+int wtd_download_history(wtd_ctx *c, int slot, double *host)
+{
+    if (!c || !host || slot < 0 || slot >= WTD_NHIST) return WTD_ERR_ARG;
+    if (slot == 0 && !c->fk_given) return WTD_ERR_STATE; /* f1 = H psi of the current state is formed lazily by the next step */
+    WTD_CU(cudaSetDevice(c->dev));
+    void *s[5];
+    ring_slots(c, s);
+    return download_array(c, s[ring_of_ref_slot(slot)], c->prec != WTD_MIXED_H32, host);
+}
+
+int wtd_upload_potentials(wtd_ctx *c, const double *host)
+{
+    if (!c || !host) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    WTD_CU(cudaMemcpyAsync(c->pots, host, 12 * (size_t)WTD_NUMEL * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    return WTD_OK;
+}
+
+int wtd_upload_occupations(wtd_ctx *c, const double *fbeta, const double *kky, const double *kkz, const int *cnt)
+{
+    if (!c || !fbeta) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    const int S = c->S;
+    double *kp2 = (double *)malloc(S * sizeof(double)), *w = (double *)malloc(S * sizeof(double));
+    for (int n = 0; n < S; n++) {
+        double ky = kky ? kky[n] : 0.0, kz = kkz ? kkz[n] : 0.0;
+#if CODEDIM == 2
+        kp2[n] = kz * kz;
+        w[n] = (fabs(kz) < 1.0e-12) ? 1.0 : 2.0;  /* +kz and -kz (cpca_dens.cu:52-58) */
+#ifdef USE_CUBIC_CUTOFF
+        if (fabs(kz + M_PI / DZ) < 1.0e-12) w[n] = 1.0;
+#endif
+#elif CODEDIM == 1
+        kp2[n] = ky * ky + kz * kz;
+        w[n] = cnt ? (double)cnt[n] : 1.0;       /* ccpca_dens.cu:47 */
+#else
+        (void)ky; (void)kz;
+        kp2[n] = 0.0;
+        w[n] = 1.0;
+#endif
+    }
+    cudaError_t e = cudaMemcpy(c->occ, fbeta, S * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->kp2, kp2, S * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->wcnt, w, S * sizeof(double), cudaMemcpyHostToDevice);
+    free(kp2); free(w);
+    return wtd_cuerr(e);
+}
+
+int wtd_initial_measurement(wtd_ctx *c, int it0)
+{
+    if (!c) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    c->it = it0;
+    c->head = 0;
+    for (int h = 0; h < WTD_NHIST; h++) WTD_CU(cudaMemsetAsync(c->hist[h], 0, c->hsz, c->st));
+    c->fk_given = 1;
+    WTD_TRY(run_pass(c, 2, true));
+    WTD_TRY(after_pass(c, true, -1));
+    return wtd_cuerr(cudaGetLastError());
+}
+
+int wtd_steps(wtd_ctx *c, int nsteps)
+{
+    if (!c || nsteps < 0) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    const bool var = WTD_VAR;
+    for (int s = 0; s < nsteps; s++) {
+        const bool last = (s == nsteps - 1);
+        if (!c->fk_given && !c->have_coef) return WTD_ERR_STATE;
+        /* predictor: f_k, y_pred, P; densities of y_pred */
+        WTD_TRY(run_pass(c, 0, var));
+        WTD_TRY(after_pass(c, var, c->it + 1));
+        /* corrector */
+        const bool g = var || last;
+        WTD_TRY(run_pass(c, 1, g));
+        WTD_TRY(after_pass(c, g, c->it + 1));
+        /* ring: f_k becomes the newest history entry, P's slot becomes free */
+        c->head = (c->head + WTD_NHIST - 1) % WTD_NHIST;
+        c->fk_given = 0;
+        c->it++;
+    }
+    return WTD_OK;
+}
+
+int wtd_energy(wtd_ctx *c, double *host11)
+{
+    if (!c || !host11) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    constexpr int N = WTD_NUMEL;
+    wslda_density D = convert_into_wslda_density(c->dens, N);
+    wslda_potential P = convert_into_wslda_potential(c->pots, N, NULL);
+    int pb = (N + 127) / 128;
+    double *e = c->ework;
+    wtd_energy_kernel<<<pb, 128, 0, c->st>>>(c->it, D, P, e + EKIN * (size_t)N, e + EPOT * (size_t)N,
+                                             e + EPAIR * (size_t)N, e + ECURRENT * (size_t)N);
+    WTD_LAUNCHED(c);
+    wtd_energy_ext_kernel<<<pb, 128, 0, c->st>>>(c->it, D, P, e);
+    WTD_LAUNCHED(c);
+#ifdef ENABLE_MODIFY_ENERGIES
+    modify_energies<<<pb, 128, 0, c->st>>>(c->it, D, P, e);
+    WTD_LAUNCHED(c);
+#endif
+    wtd_sum_items<<<TDWSLDAITEMS, 256, 0, c->st>>>(e, N, c->eout, WTD_VOLEL);
+    WTD_LAUNCHED(c);
+    WTD_CU(cudaMemcpyAsync(host11, c->eout, TDWSLDAITEMS * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    WTD_CU(cudaStreamSynchronize(c->st));
+    return WTD_OK;
+}
+
+int wtd_sync(wtd_ctx *c)
+{
+    if (!c) return WTD_ERR_ARG;
+    return wtd_cuerr(cudaStreamSynchronize(c->st));
+}
+
+int wtd_time_index(wtd_ctx *c) { return c ? c->it : 0; }
+
+int wtd_download_densities(wtd_ctx *c, double *host)
+{
+    if (!c || !host) return WTD_ERR_ARG;
+    WTD_CU(cudaMemcpyAsync(host, c->dens, 12 * (size_t)WTD_NUMEL * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    return wtd_cuerr(cudaStreamSynchronize(c->st));
+}
+
+int wtd_download_potentials(wtd_ctx *c, double *host)
+{
+    if (!c || !host) return WTD_ERR_ARG;
+    WTD_CU(cudaMemcpyAsync(host, c->pots, 12 * (size_t)WTD_NUMEL * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    return wtd_cuerr(cudaStreamSynchronize(c->st));
+}
+
+int wtd_download_qpe(wtd_ctx *c, double *host)
+{
+    if (!c || !host) return WTD_ERR_ARG;
+    WTD_CU(cudaMemcpyAsync(host, c->qpe, c->S * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    return wtd_cuerr(cudaStreamSynchronize(c->st));
+}
+
+int wtd_device_pointers(wtd_ctx *c, void **states, double **dens, double **pots)
+{
+    if (!c) return WTD_ERR_ARG;
+    if (states) *states = c->y;
+    if (dens) *dens = c->dens;
+    if (pots) *pots = c->pots;
+    return WTD_OK;
+}
+
+void *wtd_stream(wtd_ctx *c) { return c ? (void *)c->st : NULL; }
+
+int wtd_set_timing(wtd_ctx *c, int on)
+{
+    if (!c) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    if (on && !c->timing) {
+        for (int p = 0; p < 2; p++)
+            for (int k = 0; k < 2; k++)
+                for (int i = 0; i < 4096; i++) WTD_CU(cudaEventCreate(&c->ev[p][k][i]));
+    }
+    c->timing = on;
+    c->nev[0] = c->nev[1] = 0;
+    return WTD_OK;
+}
+
+int wtd_pass_times(wtd_ctx *c, double *ms_a, double *ms_b, int *count_a, int *count_b)
+{
+    if (!c || !c->timing) return WTD_ERR_STATE;
+    WTD_CU(cudaStreamSynchronize(c->st));
+    double t[2] = {0.0, 0.0};
+    for (int p = 0; p < 2; p++)
+        for (int i = 0; i < c->nev[p]; i++) {
+            float ms = 0.f;
+            WTD_CU(cudaEventElapsedTime(&ms, c->ev[p][0][i], c->ev[p][1][i]));
+            t[p] += ms;
+        }
+    if (ms_a) *ms_a = t[0];
+    if (ms_b) *ms_b = t[1];
+    if (count_a) *count_a = c->nev[0];
+    if (count_b) *count_b = c->nev[1];
+    c->nev[0] = c->nev[1] = 0;
+    return WTD_OK;
+}
+long long wtd_launch_count(wtd_ctx *c) { return c ? c->launches : 0; }
+
+} /* extern "C" */
+
+#endif

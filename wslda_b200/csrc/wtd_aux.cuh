@@ -1,0 +1,161 @@
+/*
+ * O(N) kernels that sit between the two stream passes of a step: second-stage reduction of
+ * the density slots, tau from the laplacian of rho, the per-point coefficients H psi reads,
+ * and the energy integrals.  All FP64.
+ */
+#ifndef WTD_AUX_CUH
+#define WTD_AUX_CUH
+
+#include "wtd_step.cuh"
+
+/* dens[i] = sum_s slot[s][i] / L_perp over the 12N density words (fixed slot order, so the
+ * result is bitwise reproducible).  Limited mode keeps nu, rho_a, rho_b and zeroes the rest,
+ * as kernel_calculate_densities_limited does (pca_dens.cu:133-198). */
+__global__ void wtd_dens_reduce(const double *slots, int nslots, double *dens, int N, int full, double inv_lperp)
+{
+    int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i >= 12 * N) return;
+    int q = (i < 2 * N) ? 0 : 1 + (i - 2 * N) / N; /* 0: nu, 1: rho_a, 2: tau_a, ..., 6: rho_b ... */
+    bool needed = full || q == 0 || q == 1 || q == 6;
+    double s = 0.0;
+    if (needed)
+        for (int k = 0; k < nslots; k++) s += slots[(size_t)k * 12 * N + i];
+    dens[i] = s * inv_lperp;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * single-CTA spectral operations on O(N) real fields (lattices whose field fits in smem)
+ * -------------------------------------------------------------------------------------*/
+template <class G>
+__device__ __forceinline__ void field_to_smem(double2 *B, const double *f)
+{
+    for (int p = threadIdx.x; p < G::ntot; p += blockDim.x) B[G::off(p)] = make_double2(f[p], 0.0);
+    __syncthreads();
+}
+
+/* tau_s = max(0, lap(rho_s)/2 - tau_s)  (pca_dens.cu:275-338); blockIdx.x = spin */
+template <class G>
+__global__ void wtd_tau_kernel(double *dens, const double2 *gtw, const double *gk)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *B = (double2 *)smem_raw;
+    double2 *tw = B + G::padded;
+    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    load_tables<G>(tw, kt, gtw, gk);
+    constexpr int N = G::ntot;
+    double *rho = dens + (blockIdx.x == 0 ? 2 : 7) * (size_t)N;
+    double *tau = dens + (blockIdx.x == 0 ? 3 : 8) * (size_t)N;
+    field_to_smem<G>(B, rho);
+    fft_forward<G, 1>(B, 0, tw);
+    kmul<G, OP_LAP>(B, kt);
+    __syncthreads();
+    fft_inverse<G, 1>(B, 0, tw);
+    for (int p = threadIdx.x; p < N; p += blockDim.x) {
+        double t = 0.5 * B[G::off(p)].x - tau[p];
+        if (t < 0.0) t = 0.0;
+        tau[p] = t;
+    }
+}
+
+/* per-point coefficients of H psi (see the CF_* list) from the potentials at time index it.
+ * Delta includes Delta_ext (pca_kernels.cu:271-276); constant mass uses -alpha/2, variable
+ * mass -alpha/4 (pca_kernels.cu:296-309); BdG uses -1/2 (pca_kernels.cu:478-482). */
+__global__ void wtd_prep_coef(int it, wslda_potential P, double *cf)
+{
+    int i = threadIdx.x + blockIdx.x * blockDim.x;
+    constexpr int N = WTD_NUMEL;
+    if (i >= N) return;
+    int ix, iy, iz; wtd_decode(i, ix, iy, iz);
+    Complex D = P.delta[i];
+#ifdef ENABLE_DELTA_EXT
+    D = D + WTD_D_EXT(ix, iy, iz, it, D);
+#endif
+    cf[CF_VA * N + i] = P.V_a[i] - dc_mu_a;
+    cf[CF_VB * N + i] = P.V_b[i] - dc_mu_b;
+    cf[CF_DRE * N + i] = D.real();
+    cf[CF_DIM * N + i] = D.imag();
+#if defined(BDG_MODE)
+    cf[CF_AA * N + i] = -0.5;
+    cf[CF_AB * N + i] = -0.5;
+#elif defined(FAST_CONST_EFFECTIVE_MASS_MODE)
+    cf[CF_AA * N + i] = P.alpha_a[i] * -0.5;
+    cf[CF_AB * N + i] = P.alpha_b[i] * -0.5;
+#else
+    cf[CF_AA * N + i] = P.alpha_a[i] * -0.25;
+    cf[CF_AB * N + i] = P.alpha_b[i] * -0.25;
+    cf[CF_ALA * N + i] = P.alpha_a[i];
+    cf[CF_ALB * N + i] = P.alpha_b[i];
+    cf[CF_AAX * N + i] = P.A_a_x[i];
+    cf[CF_ABX * N + i] = P.A_b_x[i];
+    cf[CF_AAY * N + i] = (CODEDIM >= 2) ? P.A_a_y[i] : 0.0;
+    cf[CF_ABY * N + i] = (CODEDIM >= 2) ? P.A_b_y[i] : 0.0;
+    cf[CF_AAZ * N + i] = (CODEDIM >= 3) ? P.A_a_z[i] : 0.0;
+    cf[CF_ABZ * N + i] = (CODEDIM >= 3) ? P.A_b_z[i] : 0.0;
+#endif
+}
+
+/* variable mass: lap(alpha_s)/4 and -div(A_s)/2 by spectral derivatives of real fields
+ * (pca_kernels.cu:778-795; pca_derivative.cu:490-700).  blockIdx.x = spin. */
+template <class G>
+__global__ void wtd_prep_var(double *cf, const double2 *gtw, const double *gk)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *B = (double2 *)smem_raw;
+    double2 *tw = B + G::padded;
+    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    load_tables<G>(tw, kt, gtw, gk);
+    constexpr int N = G::ntot;
+    const int s = blockIdx.x;
+    /* lap(alpha) */
+    field_to_smem<G>(B, cf + (s == 0 ? CF_ALA : CF_ALB) * (size_t)N);
+    fft_forward<G, 1>(B, 0, tw);
+    kmul<G, OP_LAP>(B, kt);
+    __syncthreads();
+    fft_inverse<G, 1>(B, 0, tw);
+    for (int p = threadIdx.x; p < N; p += blockDim.x) cf[(s == 0 ? CF_NA : CF_NB) * (size_t)N + p] = 0.25 * B[G::off(p)].x;
+    __syncthreads();
+    /* div A = sum_d d_d A_d */
+    double acc[64];
+    const int per = (N + blockDim.x - 1) / blockDim.x;
+    for (int k = 0; k < per && k < 64; k++) acc[k] = 0.0;
+    for (int d = 0; d < G::dims; d++) {
+        field_to_smem<G>(B, cf + ((s == 0 ? CF_AAX : CF_ABX) + d) * (size_t)N);
+        fft_forward<G, 1>(B, 0, tw);
+        if (d == 0) kmul<G, OP_DX>(B, kt);
+        else if (d == 1) kmul<G, OP_DY>(B, kt);
+        else kmul<G, OP_DZ>(B, kt);
+        __syncthreads();
+        fft_inverse<G, 1>(B, 0, tw);
+        for (int k = 0, p = threadIdx.x; p < N && k < 64; p += blockDim.x, k++) acc[k] += B[G::off(p)].x;
+        __syncthreads();
+    }
+    for (int k = 0, p = threadIdx.x; p < N && k < 64; p += blockDim.x, k++)
+        cf[(s == 0 ? CF_CJA : CF_CJB) * (size_t)N + p] = -0.5 * acc[k];
+}
+
+/* sum of each of the TDWSLDAITEMS integrand arrays (one CTA per item) */
+__global__ void wtd_sum_items(const double *e, int N, double *out, double volel)
+{
+    __shared__ double red[80];
+    double s = 0.0;
+    const double *a = e + (size_t)blockIdx.x * N;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s += a[i];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) out[blockIdx.x] = (blockIdx.x == NPARTA || blockIdx.x == NPARTB) ? s * volel : s;
+}
+
+/* FP64 <-> storage conversion of state arrays */
+template <typename T>
+__global__ void wtd_convert_in(const double2 *src, T *dst, size_t n)
+{
+    size_t i = threadIdx.x + (size_t)blockIdx.x * blockDim.x;
+    if (i < n) dst[i] = from_d<T>(src[i]);
+}
+template <typename T>
+__global__ void wtd_convert_out(const T *src, double2 *dst, size_t n)
+{
+    size_t i = threadIdx.x + (size_t)blockIdx.x * blockDim.x;
+    if (i < n) dst[i] = to_d(src[i]);
+}
+
+#endif

@@ -1,0 +1,13 @@
+/*
+ * The translation unit of one project's library (libwtd.so): the project's predefines.h and
+ * problem-definition.h are compiled together with the kernels, exactly as the reference
+ * compiles them into td-wslda-{1d,2d,3d} (hpc-engine/pca_kernels.cu:30, mk.td:114-138), so the
+ * user hooks are inlined into the device code.  Built by wslda_b200/build.py with
+ * -DCODEDIM=<1|2|3> -I<project dir>.
+ */
+#include "predefines.h"
+#include "wtd_settings.h"
+#include "wtd_surface.h"
+#include "problem-definition.h"
+#include "wtd_functional.cuh"
+#include "wtd_api.cuh"

@@ -1,0 +1,483 @@
+/*
+ * Fused TD step for states that fit in one CTA's shared memory (every 1D and 2D lattice of
+ * the reference's configurations and small 3D lattices).
+ *
+ * One persistent CTA owns one quasiparticle state (u, v) at a time and runs, for that state,
+ * everything the reference does in separate whole-array kernels:
+ *
+ *   pass A  (H y_k, predictor)     hpc-engine/pca.c:1565 (H psi into f1) + pca.c:1407-1410
+ *     FFT -> k-space multiply -> inverse FFT  (pca_derivative.cu:217-380)
+ *     (H - mu) psi with pairing coupling       (pca_kernels.cu:233-495)
+ *     <psi|H|psi> subtraction                  (pca_kernels.cu:806-833)
+ *     ABM predictor y_pred, partial corrector P (tdwslda_ode_integrator.h:26-135)
+ *     renormalisation                          (pca_kernels.cu:913-976)
+ *     density contribution of y_pred           (pca_dens.cu:13-198)
+ *   pass B  (H y_pred, corrector)  pca.c:1460-1529
+ *     same H, then y_{k+1} = P - i dt c (H - <H>) y_pred (tdwslda_ode_integrator.h:138-220),
+ *     renormalisation, density contribution (with tau and j on gradient steps).
+ *
+ * HBM traffic per state and pass is the compulsory stream: pass A reads y and the q history
+ * slots and writes f_k, y_pred and P; pass B reads y_pred and P and writes y_{k+1}.  The
+ * density sums of the states a CTA processes accumulate in a private FP64 slot (plain
+ * read-modify-write, no atomics, deterministic) that a second kernel reduces in fixed order.
+ *
+ * Precision forms (template arguments): TY = storage of y (double2 or float2), TH = storage
+ * of history and P, TC = arithmetic of the FFT and H psi.  The ABM combination, the norms,
+ * <H> and all density sums are evaluated in FP64.
+ */
+#ifndef WTD_STEP_CUH
+#define WTD_STEP_CUH
+
+#include "wtd_core.cuh"
+
+/* per-point coefficients prepared once per half-step from the potentials */
+enum {
+    CF_VA = 0,   /* V_a - mu_a                                   */
+    CF_VB,       /* V_b - mu_b                                   */
+    CF_DRE,      /* Re(Delta + Delta_ext)                        */
+    CF_DIM,      /* Im(Delta + Delta_ext)                        */
+    CF_AA,       /* -alpha_a/2 (const mass) or -alpha_a/4         */
+    CF_AB,       /* -alpha_b/2 (const mass) or -alpha_b/4         */
+    CF_NA,       /* lap(alpha_a)/4            (variable mass)     */
+    CF_NB,       /* lap(alpha_b)/4                                */
+    CF_CJA,      /* -div(A_a)/2                                   */
+    CF_CJB,      /* -div(A_b)/2                                   */
+    CF_ALA,      /* alpha_a                                       */
+    CF_ALB,      /* alpha_b                                       */
+    CF_AAX,      /* A_a x, y, z                                   */
+    CF_AAY,
+    CF_AAZ,
+    CF_ABX,      /* A_b x, y, z                                   */
+    CF_ABY,
+    CF_ABZ,
+    CF_COUNT
+};
+
+struct StepArgs {
+    void *y;            /* [2S][N] TY */
+    void *slot[5];      /* history ring, [2S][N] TH each, indexed by ring position */
+    const double *cf;   /* [CF_COUNT][N] */
+    const double *occ;  /* f_n */
+    const double *kp2;  /* per-state |k_perp|^2 of the plane-wave factor (1D/2D) */
+    const double *wcnt; /* per-state degeneracy weight */
+    double *dslot;      /* [grid][12][N] density partial sums */
+    double *qpe;        /* [S] <H> of the last H application */
+    double dt;
+    int S;
+    int fk_given;       /* pass A: f_k is already in ring slot NH-1 */
+    int accumulate;     /* add to the density slot (otherwise start from zero) */
+};
+
+/* ABM coefficients (tdwslda_ode_integrator.h:44-45, 69-70, 94-95, 153, 172, 191) */
+template <int NH> struct Abm {
+    /* predictor weights of f_k, f_{k-1}, ... */
+    __host__ __device__ static constexpr double b(int j)
+    {
+        return NH == 3 ? (j == 0 ? 23. / 12. : j == 1 ? -16. / 12. : j == 2 ? 5. / 12. : 0.)
+             : NH == 4 ? (j == 0 ? 55. / 24. : j == 1 ? -59. / 24. : j == 2 ? 37. / 24. : j == 3 ? -9. / 24. : 0.)
+                       : (j == 0 ? 1901. / 720. : j == 1 ? -2774. / 720. : j == 2 ? 2616. / 720. : j == 3 ? -1274. / 720. : 251. / 720.);
+    }
+    /* partial corrector weights of f_k, f_{k-1}, ... (the AM term of f_{k+1} is c) */
+    __host__ __device__ static constexpr double a(int j)
+    {
+        return NH == 3 ? (j == 0 ? 19. / 24. : j == 1 ? -5. / 24. : j == 2 ? 1. / 24. : 0.)
+                       : (j == 0 ? 646. / 720. : j == 1 ? -264. / 720. : j == 2 ? 106. / 720. : j == 3 ? -19. / 720. : 0.);
+    }
+    static constexpr double c = NH == 3 ? 9. / 24. : 251. / 720.;
+    static constexpr int na = NH == 3 ? 3 : 4;
+};
+
+template <typename T> __device__ __forceinline__ double2 ld2(const T *p, size_t i) { return to_d(p[i]); }
+
+/* k-space multiplier tables: per axis, wave numbers of digit-reversed positions */
+template <class G> struct KTab {
+    double k[6][128];   /* rows 0-2: k_d of a digit-reversed position; rows 3-5: same with the
+                           Nyquist mode set to 0 (first derivatives) */
+};
+
+/* the spectral operator applied in k-space */
+enum { OP_LAP = 0, OP_DX = 1, OP_DY = 2, OP_DZ = 3 };
+
+/* multiply a transformed field by the operator OP (1/N folded in): laplacian -|k|^2/N,
+ * d/dx_d -> i k_d/N with the Nyquist mode zeroed (pca_derivative.cu:152-171) */
+template <class G, int OP, typename C>
+__device__ __forceinline__ void kmul(C *buf, const double (*kt)[128])
+{
+    typedef decltype(buf[0].x) R;
+    for (int i = threadIdx.x; i < G::ntot; i += blockDim.x) {
+        int c0, c1 = 0, c2 = 0;
+        if (G::dims == 1) { c0 = i; }
+        else if (G::dims == 2) { c0 = i / G::N1; c1 = i - c0 * G::N1; }
+        else { c0 = i / (G::N1 * G::N2); int r = i - c0 * G::N1 * G::N2; c1 = r / G::N2; c2 = r - c1 * G::N2; }
+        int o = G::off(i);
+        C z = buf[o];
+        if (OP == OP_LAP) {
+            double k2 = kt[0][c0] * kt[0][c0];
+            if (G::dims >= 2) k2 += kt[1][c1] * kt[1][c1];
+            if (G::dims >= 3) k2 += kt[2][c2] * kt[2][c2];
+            R s = (R)(-1.0 * k2 / G::ntot);
+            z.x *= s; z.y *= s;
+        } else {
+            constexpr int ax = OP - 1;
+            int cc = ax == 0 ? c0 : ax == 1 ? c1 : c2;
+            R s = (R)(kt[3 + ax][cc] / G::ntot);
+            C t; t.x = -s * z.y; t.y = s * z.x;
+            z = t;
+        }
+        buf[o] = z;
+    }
+}
+
+/* ---------------------------------------------------------------------------------------
+ * shared-memory layout of the fused kernel
+ * -------------------------------------------------------------------------------------*/
+template <class G, typename TC, int NBUF> struct FusedSmem {
+    typedef typename cplx<TC>::t C;
+    static constexpr size_t buf_bytes = (size_t)G::padded * sizeof(C);
+    static constexpr size_t tw_bytes = (size_t)G::twtotal * sizeof(C);
+    static constexpr size_t bytes = NBUF * buf_bytes + tw_bytes + sizeof(KTab<G>) + 80 * sizeof(double);
+};
+
+/* load twiddles (e^{-2 pi i t/n} per axis) and the k tables into shared memory */
+template <class G, typename C>
+__device__ __forceinline__ void load_tables(C *tw, double (*kt)[128], const double2 *gtw, const double *gk)
+{
+    for (int t = threadIdx.x; t < G::twtotal; t += blockDim.x) {
+        double2 w = gtw[t];
+        C c; c.x = w.x; c.y = w.y;
+        tw[t] = c;
+    }
+    for (int t = threadIdx.x; t < 6 * 128; t += blockDim.x) kt[t / 128][t % 128] = gk[t];
+    __syncthreads();
+}
+
+/* ---------------------------------------------------------------------------------------
+ * H psi for one state, constant effective mass (FAST_CONST_EFFECTIVE_MASS_MODE / BDG_MODE).
+ * On return BU/BV hold (H psi) in natural order (compute precision) and the function returns
+ * <psi|H|psi> dV.  pca_kernels.cu:233-391 (const-mass branches) and :393-495 (BdG).
+ * -------------------------------------------------------------------------------------*/
+template <class G, typename TY, typename TC>
+__device__ __forceinline__ double hpsi_const(const TY *yu, const TY *yv, typename cplx<TC>::t *BU,
+                                             typename cplx<TC>::t *BV, const typename cplx<TC>::t *tw,
+                                             const double (*kt)[128], const double *cf, double kp2, double *red)
+{
+    typedef typename cplx<TC>::t C;
+    constexpr int N = G::ntot;
+    for (int p = threadIdx.x; p < N; p += blockDim.x) {
+        double2 u = to_d(yu[p]), v = to_d(yv[p]);
+        int o = G::off(p);
+        BU[o].x = (TC)u.x; BU[o].y = (TC)u.y;
+        BV[o].x = (TC)v.x; BV[o].y = (TC)v.y;
+    }
+    __syncthreads();
+    fft_forward<G, 2>(BU, (int)(BV - BU), tw);
+    kmul<G, OP_LAP>(BU, kt);
+    kmul<G, OP_LAP>(BV, kt);
+    __syncthreads();
+    fft_inverse<G, 2>(BU, (int)(BV - BU), tw);
+    double q = 0.0;
+    for (int p = threadIdx.x; p < N; p += blockDim.x) {
+        int o = G::off(p);
+        TC ur, ui, vr, vi;
+        {
+            double2 u = to_d(yu[p]), v = to_d(yv[p]);
+            ur = (TC)u.x; ui = (TC)u.y; vr = (TC)v.x; vi = (TC)v.y;
+        }
+        const TC va = (TC)cf[CF_VA * N + p], vb = (TC)cf[CF_VB * N + p];
+        const TC dr = (TC)cf[CF_DRE * N + p], di = (TC)cf[CF_DIM * N + p];
+        const TC aa = (TC)cf[CF_AA * N + p], ab = (TC)cf[CF_AB * N + p];
+        const TC ja = -aa * (TC)kp2, jb = -ab * (TC)kp2;
+        C lu = BU[o], lv = BV[o];
+        /* u' = (Va-mu_a+ja) u + D v + aa lap u ;  v' = -(Vb-mu_b+jb) v + D* u - ab lap v */
+        C hu, hv;
+        hu.x = (va + ja) * ur + (dr * vr - di * vi) + aa * lu.x;
+        hu.y = (va + ja) * ui + (dr * vi + di * vr) + aa * lu.y;
+        hv.x = -(vb + jb) * vr + (dr * ur + di * ui) - ab * lv.x;
+        hv.y = -(vb + jb) * vi + (dr * ui - di * ur) - ab * lv.y;
+        BU[o] = hu; BV[o] = hv;
+        q += (double)ur * (double)hu.x + (double)ui * (double)hu.y + (double)vr * (double)hv.x + (double)vi * (double)hv.y;
+    }
+    return block_sum(q, red) * WTD_DV;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * H psi for one state, variable effective mass with current corrections (ASLDA / CUSTOMEDF
+ * without SLDA_FORCE_A1).  pca_kernels.cu:233-391:
+ *   u' = (Va-mu_a+ja, cja) u + D v + (1/4)lap(alpha_a) u + sum_d (-i A_a,d) d_d u
+ *        - (1/4) alpha_a lap u - (1/4) lap(alpha_a u)
+ *   v' = -(Vb-mu_b+jb, -cjb) v + D* u - (1/4)lap(alpha_b) v - sum_d (+i A_b,d) d_d v
+ *        + (1/4) alpha_b lap v + (1/4) lap(alpha_b v)
+ * Buffers: B0 (transform of one component), W (work), HU, HV (results).
+ * -------------------------------------------------------------------------------------*/
+template <class G, typename TY, typename TC>
+__device__ __forceinline__ double hpsi_var(const TY *yu, const TY *yv, typename cplx<TC>::t *B0,
+                                           typename cplx<TC>::t *W, typename cplx<TC>::t *HU,
+                                           typename cplx<TC>::t *HV, const typename cplx<TC>::t *tw,
+                                           const double (*kt)[128], const double *cf, double kp2, double *red)
+{
+    typedef typename cplx<TC>::t C;
+    constexpr int N = G::ntot;
+    /* local terms into HU/HV */
+    for (int p = threadIdx.x; p < N; p += blockDim.x) {
+        int o = G::off(p);
+        double2 u = to_d(yu[p]), v = to_d(yv[p]);
+        double va = cf[CF_VA * N + p], vb = cf[CF_VB * N + p];
+        double dr = cf[CF_DRE * N + p], di = cf[CF_DIM * N + p];
+        double aa = cf[CF_AA * N + p], ab = cf[CF_AB * N + p];
+        double na = cf[CF_NA * N + p], nb = cf[CF_NB * N + p];
+        double cja = cf[CF_CJA * N + p], cjb = cf[CF_CJB * N + p];
+        double ja = -2.0 * aa * kp2, jb = -2.0 * ab * kp2;
+        double2 hu, hv;
+        /* (va+ja + i cja) u + D v + na u */
+        hu.x = (va + ja) * u.x - cja * u.y + (dr * v.x - di * v.y) + na * u.x;
+        hu.y = (va + ja) * u.y + cja * u.x + (dr * v.y + di * v.x) + na * u.y;
+        /* -(vb+jb - i cjb) v + D* u - nb v */
+        hv.x = -((vb + jb) * v.x + cjb * v.y) + (dr * u.x + di * u.y) - nb * v.x;
+        hv.y = -((vb + jb) * v.y - cjb * v.x) + (dr * u.y - di * u.x) - nb * v.y;
+        HU[o].x = (TC)hu.x; HU[o].y = (TC)hu.y;
+        HV[o].x = (TC)hv.x; HV[o].y = (TC)hv.y;
+    }
+    for (int comp = 0; comp < 2; comp++) {
+        const TY *y = comp == 0 ? yu : yv;
+        C *H = comp == 0 ? HU : HV;
+        const TC sgn = comp == 0 ? (TC)1 : (TC)-1;
+        __syncthreads();
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            double2 a = to_d(y[p]);
+            C c; c.x = (TC)a.x; c.y = (TC)a.y;
+            B0[G::off(p)] = c;
+        }
+        __syncthreads();
+        fft_forward<G, 1>(B0, 0, tw);
+        /* laplacian term: sgn * aa * lap */
+        for (int op = 0; op <= G::dims; op++) {
+            for (int i = threadIdx.x; i < G::padded; i += blockDim.x) W[i] = B0[i];
+            __syncthreads();
+            if (op == 0) kmul<G, OP_LAP>(W, kt);
+            else if (op == 1) kmul<G, OP_DX>(W, kt);
+            else if (op == 2) kmul<G, OP_DY>(W, kt);
+            else kmul<G, OP_DZ>(W, kt);
+            __syncthreads();
+            fft_inverse<G, 1>(W, 0, tw);
+            for (int p = threadIdx.x; p < N; p += blockDim.x) {
+                int o = G::off(p);
+                C w = W[o], h = H[o];
+                if (op == 0) {
+                    TC a = (TC)cf[(comp == 0 ? CF_AA : CF_AB) * N + p];
+                    h.x += sgn * a * w.x; h.y += sgn * a * w.y;
+                } else {
+                    /* u: + (-i A) du ; v: - (+i A) dv  ==  sgn * (-i A) * d */
+                    TC A = (TC)cf[((comp == 0 ? CF_AAX : CF_ABX) + op - 1) * N + p];
+                    h.x += sgn * (A * w.y);
+                    h.y += sgn * (-A * w.x);
+                }
+                H[o] = h;
+            }
+        }
+        /* - (1/4) lap(alpha psi) with the spin's sign */
+        __syncthreads();
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            double2 a = to_d(y[p]);
+            TC al = (TC)cf[(comp == 0 ? CF_ALA : CF_ALB) * N + p];
+            C c; c.x = (TC)a.x * al; c.y = (TC)a.y * al;
+            W[G::off(p)] = c;
+        }
+        __syncthreads();
+        fft_forward<G, 1>(W, 0, tw);
+        kmul<G, OP_LAP>(W, kt);
+        __syncthreads();
+        fft_inverse<G, 1>(W, 0, tw);
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            int o = G::off(p);
+            C w = W[o], h = H[o];
+            h.x += sgn * (TC)(-0.25) * w.x; h.y += sgn * (TC)(-0.25) * w.y;
+            H[o] = h;
+        }
+    }
+    __syncthreads();
+    double q = 0.0;
+    for (int p = threadIdx.x; p < N; p += blockDim.x) {
+        int o = G::off(p);
+        double2 u = to_d(yu[p]), v = to_d(yv[p]);
+        C hu = HU[o], hv = HV[o];
+        q += u.x * (double)hu.x + u.y * (double)hu.y + v.x * (double)hv.x + v.y * (double)hv.y;
+    }
+    return block_sum(q, red) * WTD_DV;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * density contribution of one normalised state (pca_dens.cu:13-198, cpca_dens.cu:14-140,
+ * ccpca_dens.cu:14-140).  Limited form: rho_a, rho_b, nu.  The slot has the reference's
+ * 12-block layout [nu re/im interleaved, rho_a, tau_a, j_a xyz, rho_b, tau_b, j_b xyz].
+ * -------------------------------------------------------------------------------------*/
+__device__ __forceinline__ void dens_limited(double *ds, int p, int N, double2 u, double2 v, double f, double w)
+{
+    double fa = f * w, fb = (1.0 - f) * w, fn = (1.0 - 2.0 * f) * 0.5 * w;
+    ds[2 * p] += (u.x * v.x + u.y * v.y) * fn;
+    ds[2 * p + 1] += (u.y * v.x - u.x * v.y) * fn;
+    ds[2 * (size_t)N + p] += (u.x * u.x + u.y * u.y) * fa;
+    ds[7 * (size_t)N + p] += (v.x * v.x + v.y * v.y) * fb;
+}
+
+/* tau and j contributions of one normalised component (pca_dens.cu:41-108).  B0 holds the
+ * component in natural order and is transformed in place; W is work; ysrc gives the stored
+ * normalised values.  tau_tmp_s += f_s Re(conj(psi)(lap psi - |k_perp|^2 psi)),
+ * j_s,d += (+1 for u, -1 for v) f_s Im(conj(psi) d_d psi). */
+template <class G, typename TY, typename TC>
+__device__ __forceinline__ void dens_gradients(double *ds, const TY *ysrc, typename cplx<TC>::t *B0,
+                                               typename cplx<TC>::t *W, const typename cplx<TC>::t *tw,
+                                               const double (*kt)[128], double f, double w, double kp2, int comp)
+{
+    typedef typename cplx<TC>::t C;
+    constexpr int N = G::ntot;
+    const double fw = (comp == 0 ? f : (1.0 - f)) * w;
+    const int tau_q = comp == 0 ? 3 : 8, j_q = comp == 0 ? 4 : 9;
+    const double jsgn = comp == 0 ? 1.0 : -1.0;
+    __syncthreads();
+    fft_forward<G, 1>(B0, 0, tw);
+    for (int op = 0; op <= G::dims; op++) {
+        for (int i = threadIdx.x; i < G::padded; i += blockDim.x) W[i] = B0[i];
+        __syncthreads();
+        if (op == 0) kmul<G, OP_LAP>(W, kt);
+        else if (op == 1) kmul<G, OP_DX>(W, kt);
+        else if (op == 2) kmul<G, OP_DY>(W, kt);
+        else kmul<G, OP_DZ>(W, kt);
+        __syncthreads();
+        fft_inverse<G, 1>(W, 0, tw);
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            double2 sv = to_d(ysrc[p]);
+            C d = W[G::off(p)];
+            double dx = d.x, dy = d.y;
+            if (op == 0) {
+                double lx = dx - sv.x * kp2, ly = dy - sv.y * kp2;
+                ds[tau_q * (size_t)N + p] += (sv.x * lx + sv.y * ly) * fw;
+            } else {
+                ds[(j_q + op - 1) * (size_t)N + p] += jsgn * (sv.x * dy - sv.y * dx) * fw;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+/* ---------------------------------------------------------------------------------------
+ * the fused pass kernel
+ *   PASS 0 (A): f_k = (H - <H>) y (or read), predictor, P, renormalise, densities of y_pred
+ *   PASS 1 (B): f = (H - <H>) y_pred, y = P - i dt c f, renormalise, densities
+ * VAR: variable effective mass; GRAD: tau and j of the output state too.
+ * -------------------------------------------------------------------------------------*/
+template <class G, typename TY, typename TH, typename TC, int NH, int PASS, bool VAR, bool GRAD>
+__global__ void __launch_bounds__(512, 1)
+wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
+{
+    typedef typename cplx<TC>::t C;
+    constexpr int N = G::ntot;
+    constexpr int NBUF = VAR ? 4 : (GRAD ? 3 : 2);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *BU = (C *)smem_raw;
+    C *BV = BU + G::padded;
+    C *B2 = BV + G::padded;
+    C *B3 = B2 + G::padded;
+    C *tw = BU + NBUF * G::padded;
+    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    double *red = (double *)(kt + 6);
+
+    load_tables<G>(tw, kt, gtw, gk);
+
+    TY *Y = (TY *)a.y;
+    double *ds = a.dslot + (size_t)blockIdx.x * 12 * N;
+    if (!a.accumulate)
+        for (int i = threadIdx.x; i < 12 * N; i += blockDim.x) ds[i] = 0.0;
+    const double dt = a.dt;
+    const size_t SN = (size_t)a.S * N;
+
+    for (int n = blockIdx.x; n < a.S; n += gridDim.x) {
+        TY *yu = Y + (size_t)n * N, *yv = Y + SN + (size_t)n * N;
+        const double kp2 = a.kp2[n];
+        /* results of H land in (HU, HV) */
+        C *HU = VAR ? B2 : BU, *HV = VAR ? B3 : BV;
+        double E = 0.0;
+        const bool haveH = (PASS == 1) || (PASS == 0 && !a.fk_given);
+        if (haveH) {
+            if (VAR) E = hpsi_var<G, TY, TC>(yu, yv, BU, BV, HU, HV, tw, kt, a.cf, kp2, red);
+            else E = hpsi_const<G, TY, TC>(yu, yv, BU, BV, tw, kt, a.cf, kp2, red);
+            if (threadIdx.x == 0) a.qpe[n] = E;
+        }
+        /* ---- ABM update, unnormalised result into (HU, HV) ---- */
+        double nrm = 0.0;
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            const int o = G::off(p);
+#pragma unroll
+            for (int comp = 0; comp < 2; comp++) {
+                const size_t gi = (comp ? SN : 0) + (size_t)n * N + p;
+                double2 y0 = to_d(Y[gi]);
+                double2 fk = make_double2(0.0, 0.0);
+                if (PASS == 2) {
+                    /* initial measurement: normalise only (pca.c:941) */
+                } else if (haveH) {
+                    C h = comp ? HV[o] : HU[o];
+                    fk.x = (double)h.x - E * y0.x;
+                    fk.y = (double)h.y - E * y0.y;
+                } else {
+                    fk = ld2((const TH *)a.slot[NH - 1], gi);
+                }
+                double2 out;
+                if (PASS == 2) {
+                    out = y0;
+                } else if (PASS == 0) {
+                    typedef Abm<NH> A;
+                    /* sums in the reference's order: f_k*b0 - f_{k-1}*|b1| + ... */
+                    double2 sb = make_double2(fk.x * A::b(0), fk.y * A::b(0));
+                    double2 sa = make_double2(fk.x * A::a(0), fk.y * A::a(0));
+#pragma unroll
+                    for (int j = 1; j < NH; j++) {
+                        double2 fj = ld2((const TH *)a.slot[j - 1], gi);
+                        sb.x += fj.x * A::b(j); sb.y += fj.y * A::b(j);
+                        if (j < A::na) { sa.x += fj.x * A::a(j); sa.y += fj.y * A::a(j); }
+                    }
+                    /* y_pred = y + (-i dt) sb ; P = y + (-i dt) sa */
+                    out.x = y0.x + dt * sb.y; out.y = y0.y - dt * sb.x;
+                    double2 P = make_double2(y0.x + dt * sa.y, y0.y - dt * sa.x);
+                    if (haveH) ((TH *)a.slot[NH - 1])[gi] = from_d<TH>(fk);
+                    ((TH *)a.slot[NH - 2])[gi] = from_d<TH>(P);
+                } else {
+                    /* y = (-i dt) f c + P */
+                    double2 P = ld2((const TH *)a.slot[NH - 2], gi);
+                    const double c = Abm<NH>::c;
+                    out.x = dt * fk.y * c + P.x;
+                    out.y = -dt * fk.x * c + P.y;
+                }
+                nrm += out.x * out.x + out.y * out.y;
+                C r; r.x = (TC)out.x; r.y = (TC)out.y;
+                if (comp) HV[o] = r; else HU[o] = r;
+            }
+        }
+        const double c = 1.0 / sqrt(block_sum(nrm, red) * WTD_DV);
+        /* ---- normalise, store, densities ---- */
+        const double f = a.occ[n], w = a.wcnt[n];
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            const int o = G::off(p);
+            C hu = HU[o], hv = HV[o];
+            double2 u = make_double2((double)hu.x * c, (double)hu.y * c);
+            double2 v = make_double2((double)hv.x * c, (double)hv.y * c);
+            TY su = from_d<TY>(u), sv = from_d<TY>(v);
+            yu[p] = su; yv[p] = sv;
+            u = to_d(su); v = to_d(sv);
+            dens_limited(ds, p, N, u, v, f, w);
+            if (GRAD) {
+                C cu, cv;
+                cu.x = (TC)u.x; cu.y = (TC)u.y; cv.x = (TC)v.x; cv.y = (TC)v.y;
+                HU[o] = cu; HV[o] = cv;
+            }
+        }
+        if (GRAD) {
+            /* const mass: (HU, HV) = (BU, BV) hold the state, B2 is work.
+             * variable mass: (HU, HV) = (B2, B3), BU is work. */
+            C *Wk = VAR ? BU : B2;
+            dens_gradients<G, TY, TC>(ds, yu, HU, Wk, tw, kt, f, w, kp2, 0);
+            dens_gradients<G, TY, TC>(ds, yv, HV, Wk, tw, kt, f, w, kp2, 1);
+        }
+        __syncthreads();
+    }
+}
+
+#endif
