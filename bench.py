@@ -86,7 +86,7 @@ class ClockSampler:
         sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
         mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if "Active" in s[3 + k]})
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 
@@ -131,7 +131,7 @@ def run_wtd(args, rank, world):
     from wslda_b200 import TDRun
     wl = WORKLOADS[args.workload]
     name = wl["project"]
-    nwf_total = wl["nwf"]
+    nwf_total = args.nwf or wl["nwf"]
     nwf = nwf_total // world  # states sharded over ranks; per-rank work fixed by the config
     torch.cuda.set_device(rank % max(1, torch.cuda.device_count()))
     dev = torch.cuda.current_device()
@@ -239,6 +239,7 @@ def main():
     ap.add_argument("--impl", default="wtd", choices=["wtd", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--fp64-only", action="store_true")
+    ap.add_argument("--nwf", type=int, default=0, help="override the workload's state count (small profiling cases)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-refcuda", action="store_true")
     args = ap.parse_args()
@@ -247,7 +248,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     wl = WORKLOADS[args.workload]
     metric = "qp-state*steps/s"
-    cfg = {"workload": wl["desc"], "project": wl["project"], "states": wl["nwf"], "precision": "fp64",
+    cfg = {"workload": wl["desc"], "project": wl["project"], "states": args.nwf or wl["nwf"], "precision": "fp64",
            "l2": "inputs larger than L2 (state arrays of GBs)", "parallelism": f"states sharded over {world} GPU(s)"}
 
     if args.impl == "reference":

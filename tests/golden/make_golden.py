@@ -61,6 +61,28 @@ def state_moments(y, nwf, n):
                      (a[0] @ ramp).real, (a[0] @ ramp).imag, (a[1] @ ramp).real, (a[1] @ ramp).imag], 1)
 
 
+MAX_POINTS = 2048
+
+
+def point_sample(n):
+    """Lattice points kept for fields of large lattices (fixed, seeded, sorted)."""
+    if n <= MAX_POINTS:
+        return np.arange(n)
+    return np.sort(np.random.Generator(np.random.PCG64(12345)).choice(n, MAX_POINTS, replace=False))
+
+
+def slim(rec, n):
+    """Keep the 12 density and 12 potential blocks only at point_sample(n) for large lattices."""
+    idx = point_sample(n)
+    if idx.size == n:
+        return rec
+    for key in ("densities", "potentials"):
+        blocks = rec[key].reshape(12, n)
+        rec[key] = np.ascontiguousarray(blocks[:, idx]).reshape(-1)
+    rec["points"] = idx
+    return rec
+
+
 def run_case(name, out_dir):
     nwf, nsteps, nmeas, full = CASES[name]
     proj, y0, occ, pots, params, extra = case_inputs(name, nwf)
@@ -95,6 +117,7 @@ def run_case(name, out_dir):
     if full:
         rec["states"] = y
         rec["history0"] = hist[:M]
+    rec = slim(rec, n)
     path = os.path.join(out_dir, f"{name}.npz")
     np.savez_compressed(path, **rec)
     print(f"{name}: nwf={nwf} steps={nsteps}x{nmeas} E={en[:7].sum():.12g} N={en[7]:.12g},{en[8]:.12g} "
@@ -104,8 +127,18 @@ def run_case(name, out_dir):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--slim-existing", action="store_true", help="apply slim() to fixtures in --out")
     ap.add_argument("projects", nargs="*")
     a = ap.parse_args()
+    if a.slim_existing:
+        for name in (a.projects or list(CASES)):
+            path = os.path.join(a.out, f"{name}.npz")
+            if os.path.exists(path):
+                rec = dict(np.load(path))
+                n = P.Project(name).numel
+                if "points" not in rec:
+                    np.savez_compressed(path, **slim(rec, n))
+        return
     os.makedirs(a.out, exist_ok=True)
     for name in (a.projects or list(CASES)):
         run_case(name, a.out)

@@ -38,7 +38,7 @@ def run_gpu(name, nwf, nsteps, nmeas=1, precision=0, inp=None):
     for _ in range(nmeas):
         r.steps(nsteps)
     out = dict(states=r.states(), densities=r.densities(), potentials=r.potentials(), energy=r.energy(),
-               qpe=r.qpe(), launches=r.launches())
+               qpe=r.qpe(), history0=r.history(0), launches=r.launches())
     r.close()
     return out
 

@@ -29,6 +29,7 @@ def _compare(name, nwf, nsteps, nmeas, tol=TOL):
             assert abs(E_g[k] - E_o[k]) / scale < tol, f"{name} energy[{k}] {E_g[k]!r} vs {E_o[k]!r}"
     assert rel(g["qpe"], o["qpe"]) < tol
     assert rel(g["states"], o["states"]) < tol
+    assert rel(g["history0"], o["history"][0]) < tol
     assert g["launches"] > 0
 
 

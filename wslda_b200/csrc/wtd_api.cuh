@@ -45,6 +45,7 @@ struct wtd_ctx {
     void *extra;
     size_t extra_bytes;
     int grid;
+    int block;                  /* threads per CTA of the fused passes on large lattices */
     int it;
     int fk_given;
     int have_coef;
@@ -78,14 +79,24 @@ static int launch_pass_t(wtd_ctx *c, StepArgs &a)
     constexpr size_t sm = fused_smem<TC, NBUF>();
     if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     else {
-        auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD>;
-        static bool attr = false;
-        if (!attr) {
-            WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            attr = true;
+        if (c->block == 1024 && WG::ntot >= 2048) {
+            auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD, 1024>;
+            static bool attr = false;
+            if (!attr) {
+                WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                attr = true;
+            }
+            k<<<c->grid, 1024, sm, c->st>>>(a, c->tw, c->ktab);
+        } else {
+            auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD, 512>;
+            static bool attr = false;
+            if (!attr) {
+                WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                attr = true;
+            }
+            int threads = WG::ntot >= 512 ? 512 : ((WG::ntot + 31) / 32) * 32;
+            k<<<c->grid, threads, sm, c->st>>>(a, c->tw, c->ktab);
         }
-        int threads = WG::ntot >= 512 ? 512 : ((WG::ntot + 31) / 32) * 32;
-        k<<<c->grid, threads, sm, c->st>>>(a, c->tw, c->ktab);
         WTD_LAUNCHED(c);
     }
     return WTD_OK;
@@ -130,7 +141,19 @@ static int run_pass(wtd_ctx *c, int pass, bool grad)
     }
     if (pass == 0) return grad ? launch_pass<0, true>(c, a) : launch_pass<0, false>(c, a);
     if (pass == 1) return grad ? launch_pass<1, true>(c, a) : launch_pass<1, false>(c, a);
+    if (pass == 3) return launch_pass<3, false>(c, a);
     return grad ? launch_pass<2, true>(c, a) : launch_pass<2, false>(c, a);
+}
+
+/* f1 = (H - <H>) psi of the current state and its quasiparticle energies, as the reference
+ * leaves them after a step (pca.c:1565, d_workarea[0..n)); later steps reuse f1 */
+static int ensure_fk(wtd_ctx *c)
+{
+    if (c->fk_given) return WTD_OK;
+    if (!c->have_coef) return WTD_ERR_STATE;
+    WTD_TRY(run_pass(c, 3, false));
+    c->fk_given = 1;
+    return WTD_OK;
 }
 
 /* densities from the slots, tau, potentials and H coefficients at time index it */
@@ -166,12 +189,40 @@ static int after_pass(wtd_ctx *c, bool full, int it)
         if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
         static bool attr = false;
         if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_prep_var<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
-        wtd_prep_var<WG><<<2, 1024, sm, c->st>>>(c->cf, c->tw, c->ktab);
+        wtd_prep_var<WG><<<2, 256, sm, c->st>>>(c->cf, c->tw, c->ktab);
         WTD_LAUNCHED(c);
     }
 #endif
     c->have_coef = 1;
     return WTD_OK;
+}
+
+template <typename TY, typename TH, typename TC>
+static int occupancy_t(int block)
+{
+    constexpr int NBUF = WTD_VAR ? 4 : 3;
+    constexpr size_t sm = fused_smem<TC, NBUF>();
+    if (sm > WTD_SMEM_MAX) return 1;
+    int nb = 1;
+    if (block == 1024 && WG::ntot >= 2048) {
+        auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, 1, WTD_VAR, true, 1024>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 1024, sm);
+    } else {
+        auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, 1, WTD_VAR, true, 512>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        int threads = WG::ntot >= 512 ? 512 : ((WG::ntot + 31) / 32) * 32;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, sm);
+    }
+    cudaGetLastError();
+    return nb < 1 ? 1 : (nb > 16 ? 16 : nb);
+}
+
+static int occupancy_per_sm(wtd_ctx *c)
+{
+    if (c->prec == WTD_FP64) return occupancy_t<double2, double2, double>(c->block);
+    if (c->prec == WTD_MIXED_H64) return occupancy_t<float2, double2, float>(c->block);
+    return occupancy_t<float2, float2, float>(c->block);
 }
 
 /* ---------------------------------------------------------------------------------------
@@ -223,17 +274,14 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     c->hsz = n2 * elem_bytes_h(precision);
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-    /* one resident CTA per SM for the 2-D fused pass; more for tiny lattices */
-    int per_sm = 1;
+    c->block = 512;
     {
-        size_t sm = (precision == WTD_FP64) ? fused_smem<double, WTD_VAR ? 4 : 3>() : fused_smem<float, WTD_VAR ? 4 : 3>();
-        per_sm = (int)(200000 / (sm + 1024));
-        int thr = WG::ntot >= 512 ? 512 : ((WG::ntot + 31) / 32) * 32;
-        int by_thr = 2048 / thr;
-        if (per_sm > by_thr) per_sm = by_thr;
-        if (per_sm > 8) per_sm = 8;
-        if (per_sm < 1) per_sm = 1;
+        const char *b = getenv("WTD_BLOCK");
+        if (b && atoi(b) == 1024) c->block = 1024;
     }
+    /* persistent grid: as many CTAs as fit on every SM for the most demanding pass variant
+     * (the gradient pass), so all variants of a run share one slot layout */
+    int per_sm = occupancy_per_sm(c);
     c->grid = nsm * per_sm;
     if (c->grid > nwf) c->grid = nwf;
     cudaError_t e = cudaSuccess;
@@ -434,8 +482,8 @@ int wtd_upload_history(wtd_ctx *c, int slot, const double *host)
 int wtd_download_history(wtd_ctx *c, int slot, double *host)
 {
     if (!c || !host || slot < 0 || slot >= WTD_NHIST) return WTD_ERR_ARG;
-    if (slot == 0 && !c->fk_given) return WTD_ERR_STATE; /* f1 = H psi of the current state is formed lazily by the next step */
     WTD_CU(cudaSetDevice(c->dev));
+    if (slot == 0) WTD_TRY(ensure_fk(c));
     void *s[5];
     ring_slots(c, s);
     return download_array(c, s[ring_of_ref_slot(slot)], c->prec != WTD_MIXED_H32, host);
@@ -565,6 +613,8 @@ int wtd_download_potentials(wtd_ctx *c, double *host)
 int wtd_download_qpe(wtd_ctx *c, double *host)
 {
     if (!c || !host) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    WTD_TRY(ensure_fk(c));
     WTD_CU(cudaMemcpyAsync(host, c->qpe, c->S * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     return wtd_cuerr(cudaStreamSynchronize(c->st));
 }

@@ -35,7 +35,7 @@ __device__ __forceinline__ void field_to_smem(double2 *B, const double *f)
 
 /* tau_s = max(0, lap(rho_s)/2 - tau_s)  (pca_dens.cu:275-338); blockIdx.x = spin */
 template <class G>
-__global__ void wtd_tau_kernel(double *dens, const double2 *gtw, const double *gk)
+__global__ void __launch_bounds__(512) wtd_tau_kernel(double *dens, const double2 *gtw, const double *gk)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *B = (double2 *)smem_raw;
@@ -97,7 +97,7 @@ __global__ void wtd_prep_coef(int it, wslda_potential P, double *cf)
 /* variable mass: lap(alpha_s)/4 and -div(A_s)/2 by spectral derivatives of real fields
  * (pca_kernels.cu:778-795; pca_derivative.cu:490-700).  blockIdx.x = spin. */
 template <class G>
-__global__ void wtd_prep_var(double *cf, const double2 *gtw, const double *gk)
+__global__ void __launch_bounds__(256) wtd_prep_var(double *cf, const double2 *gtw, const double *gk)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *B = (double2 *)smem_raw;

@@ -160,14 +160,15 @@ template <int SIGN, int R, typename C> __device__ __forceinline__ void dft_r(C *
  * Forward (SIGN=-1): DIF butterfly then twiddle w_L^{jq}.  Inverse (SIGN=+1): multiply by
  * conj(w_L^{jq}), then the inverse butterfly — the exact reverse of the forward stage.
  * -------------------------------------------------------------------------------------*/
-template <class G, int AX, int L, int R, int SIGN, typename C>
-__device__ __forceinline__ void fft_stage(C *buf, const C *tw)
+template <class G, int AX, int L, int R, int SIGN, int NF, typename C>
+__device__ __forceinline__ void fft_stage(C *buf, int fstride, const C *tw)
 {
     constexpr int n = G::n(AX);
     constexpr int m = L / R;
     constexpr int nbfly = G::ntot / R;
     constexpr int twmul = n / L;
     constexpr bool fast = (AX == G::dims - 1);
+    constexpr int st = fast ? 1 : (AX == 0 ? (G::ntot / G::N0 / G::nfast) * G::pitch : G::pitch);
     for (int b = threadIdx.x; b < nbfly; b += blockDim.x) {
         int j, s, lineoff;
         if (fast) {
@@ -189,28 +190,37 @@ __device__ __forceinline__ void fft_stage(C *buf, const C *tw)
                 lineoff = x * G::N1 * G::pitch + pad_index(z);
             }
         }
-        constexpr int st = fast ? 1 : (AX == 0 ? (G::ntot / G::N0 / G::nfast) * G::pitch : G::pitch);
-        C v[R];
         const int base = s * L + j;
+        int addr[R];
 #pragma unroll
         for (int q = 0; q < R; q++) {
             int e = base + q * m;
-            v[q] = buf[fast ? lineoff + pad_index(e) : lineoff + e * st];
+            addr[q] = fast ? lineoff + pad_index(e) : lineoff + e * st;
         }
-        if (SIGN > 0) {
+        C v[NF][R];
 #pragma unroll
-            for (int q = 1; q < R; q++) v[q] = cmulc(v[q], tw[(j * q * twmul) % n]);
-            dft_r<SIGN, R>(v);
-        } else {
-            dft_r<SIGN, R>(v);
+        for (int f = 0; f < NF; f++)
 #pragma unroll
-            for (int q = 1; q < R; q++) v[q] = cmul(v[q], tw[(j * q * twmul) % n]);
+            for (int q = 0; q < R; q++) v[f][q] = buf[f * fstride + addr[q]];
+        C w[R];
+#pragma unroll
+        for (int q = 1; q < R; q++) w[q] = tw[(j * q * twmul) % n];
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+            if (SIGN > 0) {
+#pragma unroll
+                for (int q = 1; q < R; q++) v[f][q] = cmulc(v[f][q], w[q]);
+                dft_r<SIGN, R>(v[f]);
+            } else {
+                dft_r<SIGN, R>(v[f]);
+#pragma unroll
+                for (int q = 1; q < R; q++) v[f][q] = cmul(v[f][q], w[q]);
+            }
         }
 #pragma unroll
-        for (int q = 0; q < R; q++) {
-            int e = base + q * m;
-            buf[fast ? lineoff + pad_index(e) : lineoff + e * st] = v[q];
-        }
+        for (int f = 0; f < NF; f++)
+#pragma unroll
+            for (int q = 0; q < R; q++) buf[f * fstride + addr[q]] = v[f][q];
     }
 }
 
@@ -220,8 +230,7 @@ __device__ __forceinline__ void fft_axis_fwd(C *buf, int fstride, const C *tw)
 {
     if constexpr (L > 1) {
         constexpr int R = radix_first(L);
-#pragma unroll
-        for (int f = 0; f < NF; f++) fft_stage<G, AX, L, R, -1>(buf + f * fstride, tw);
+        fft_stage<G, AX, L, R, -1, NF>(buf, fstride, tw);
         __syncthreads();
         fft_axis_fwd<G, AX, S + 1, L / R, NF>(buf, fstride, tw);
     }
@@ -233,8 +242,7 @@ __device__ __forceinline__ void fft_axis_inv(C *buf, int fstride, const C *tw)
     if constexpr (L > 1) {
         constexpr int R = radix_first(L);
         fft_axis_inv<G, AX, L / R, NF>(buf, fstride, tw);
-#pragma unroll
-        for (int f = 0; f < NF; f++) fft_stage<G, AX, L, R, +1>(buf + f * fstride, tw);
+        fft_stage<G, AX, L, R, +1, NF>(buf, fstride, tw);
         __syncthreads();
     }
 }
@@ -256,6 +264,48 @@ __device__ __forceinline__ void fft_inverse(C *buf, int fstride, const C *twtab)
     if constexpr (G::dims >= 2) fft_axis_inv<G, 1, G::N1, NF>(buf, fstride, twtab + G::twoff(1));
     fft_axis_inv<G, 0, G::N0, NF>(buf, fstride, twtab + G::twoff(0));
 }
+
+/* ---------------------------------------------------------------------------------------
+ * asynchronous L2 prefetch of a contiguous range (sm_90+ bulk prefetch, no registers or
+ * shared memory used; completion is not tracked — later ordinary loads simply hit L2).
+ * addr and bytes must be multiples of 16.
+ * -------------------------------------------------------------------------------------*/
+__device__ __forceinline__ void prefetch_l2(const void *addr, size_t bytes)
+{
+    const char *p = (const char *)addr;
+    while (bytes > 0) {
+        unsigned chunk = bytes > 32768 ? 32768u : (unsigned)bytes;
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(chunk) : "memory");
+        p += chunk;
+        bytes -= chunk;
+    }
+}
+
+/* L2 residency policies (createpolicy): data reused across states — the per-CTA density
+ * slots and the per-point H coefficients — is kept (evict_last) while the state stream passes
+ * through (evict_first / .cs) */
+__device__ __forceinline__ uint64_t l2_policy_keep()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ double ld_keep(const double *a, uint64_t pol)
+{
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_keep(double *a, double v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
+
+/* streaming loads/stores (evict-first): state and history arrays are touched once per pass */
+__device__ __forceinline__ double2 ld_stream(const double2 *p) { return __ldcs(p); }
+__device__ __forceinline__ float2 ld_stream(const float2 *p) { return __ldcs(p); }
+__device__ __forceinline__ void st_stream(double2 *p, double2 v) { __stcs(p, v); }
+__device__ __forceinline__ void st_stream(float2 *p, float2 v) { __stcs(p, v); }
 
 /* ---------------------------------------------------------------------------------------
  * reductions

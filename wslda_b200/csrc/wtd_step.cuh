@@ -163,6 +163,7 @@ __device__ __forceinline__ double hpsi_const(const TY *yu, const TY *yv, typenam
 {
     typedef typename cplx<TC>::t C;
     constexpr int N = G::ntot;
+    const uint64_t pol = l2_policy_keep();
     for (int p = threadIdx.x; p < N; p += blockDim.x) {
         double2 u = to_d(yu[p]), v = to_d(yv[p]);
         int o = G::off(p);
@@ -183,9 +184,9 @@ __device__ __forceinline__ double hpsi_const(const TY *yu, const TY *yv, typenam
             double2 u = to_d(yu[p]), v = to_d(yv[p]);
             ur = (TC)u.x; ui = (TC)u.y; vr = (TC)v.x; vi = (TC)v.y;
         }
-        const TC va = (TC)cf[CF_VA * N + p], vb = (TC)cf[CF_VB * N + p];
-        const TC dr = (TC)cf[CF_DRE * N + p], di = (TC)cf[CF_DIM * N + p];
-        const TC aa = (TC)cf[CF_AA * N + p], ab = (TC)cf[CF_AB * N + p];
+        const TC va = (TC)ld_keep(cf + CF_VA * N + p, pol), vb = (TC)ld_keep(cf + CF_VB * N + p, pol);
+        const TC dr = (TC)ld_keep(cf + CF_DRE * N + p, pol), di = (TC)ld_keep(cf + CF_DIM * N + p, pol);
+        const TC aa = (TC)ld_keep(cf + CF_AA * N + p, pol), ab = (TC)ld_keep(cf + CF_AB * N + p, pol);
         const TC ja = -aa * (TC)kp2, jb = -ab * (TC)kp2;
         C lu = BU[o], lv = BV[o];
         /* u' = (Va-mu_a+ja) u + D v + aa lap u ;  v' = -(Vb-mu_b+jb) v + D* u - ab lap v */
@@ -266,10 +267,10 @@ __device__ __forceinline__ double hpsi_var(const TY *yu, const TY *yv, typename 
                     TC a = (TC)cf[(comp == 0 ? CF_AA : CF_AB) * N + p];
                     h.x += sgn * a * w.x; h.y += sgn * a * w.y;
                 } else {
-                    /* u: + (-i A) du ; v: - (+i A) dv  ==  sgn * (-i A) * d */
+                    /* u: + (-i A_a) du ; v: - (+i A_b) dv, i.e. the same form (-i A) d for both */
                     TC A = (TC)cf[((comp == 0 ? CF_AAX : CF_ABX) + op - 1) * N + p];
-                    h.x += sgn * (A * w.y);
-                    h.y += sgn * (-A * w.x);
+                    h.x += A * w.y;
+                    h.y += -A * w.x;
                 }
                 H[o] = h;
             }
@@ -310,13 +311,15 @@ __device__ __forceinline__ double hpsi_var(const TY *yu, const TY *yv, typename 
  * ccpca_dens.cu:14-140).  Limited form: rho_a, rho_b, nu.  The slot has the reference's
  * 12-block layout [nu re/im interleaved, rho_a, tau_a, j_a xyz, rho_b, tau_b, j_b xyz].
  * -------------------------------------------------------------------------------------*/
-__device__ __forceinline__ void dens_limited(double *ds, int p, int N, double2 u, double2 v, double f, double w)
+__device__ __forceinline__ void dens_limited(double *ds, int p, int N, double2 u, double2 v, double f, double w, uint64_t pol)
 {
     double fa = f * w, fb = (1.0 - f) * w, fn = (1.0 - 2.0 * f) * 0.5 * w;
-    ds[2 * p] += (u.x * v.x + u.y * v.y) * fn;
-    ds[2 * p + 1] += (u.y * v.x - u.x * v.y) * fn;
-    ds[2 * (size_t)N + p] += (u.x * u.x + u.y * u.y) * fa;
-    ds[7 * (size_t)N + p] += (v.x * v.x + v.y * v.y) * fb;
+    double *a0 = ds + 2 * p, *a1 = ds + 2 * p + 1, *a2 = ds + 2 * (size_t)N + p, *a3 = ds + 7 * (size_t)N + p;
+    double s0 = ld_keep(a0, pol), s1 = ld_keep(a1, pol), s2 = ld_keep(a2, pol), s3 = ld_keep(a3, pol);
+    st_keep(a0, s0 + (u.x * v.x + u.y * v.y) * fn, pol);
+    st_keep(a1, s1 + (u.y * v.x - u.x * v.y) * fn, pol);
+    st_keep(a2, s2 + (u.x * u.x + u.y * u.y) * fa, pol);
+    st_keep(a3, s3 + (v.x * v.x + v.y * v.y) * fb, pol);
 }
 
 /* tau and j contributions of one normalised component (pca_dens.cu:41-108).  B0 holds the
@@ -363,10 +366,13 @@ __device__ __forceinline__ void dens_gradients(double *ds, const TY *ysrc, typen
  * the fused pass kernel
  *   PASS 0 (A): f_k = (H - <H>) y (or read), predictor, P, renormalise, densities of y_pred
  *   PASS 1 (B): f = (H - <H>) y_pred, y = P - i dt c f, renormalise, densities
+ *   PASS 2    : renormalise and densities only (initial measurement, pca.c:939-958)
+ *   PASS 3    : f = (H - <H>) y into ring slot NH-1 only — the reference's end-of-step
+ *               apply_hamiltonian into f1 (pca.c:1565), formed on demand
  * VAR: variable effective mass; GRAD: tau and j of the output state too.
  * -------------------------------------------------------------------------------------*/
-template <class G, typename TY, typename TH, typename TC, int NH, int PASS, bool VAR, bool GRAD>
-__global__ void __launch_bounds__(512, 1)
+template <class G, typename TY, typename TH, typename TC, int NH, int PASS, bool VAR, bool GRAD, int BS>
+__global__ void __launch_bounds__(BS, 1)
 wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
 {
     typedef typename cplx<TC>::t C;
@@ -384,45 +390,102 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
     load_tables<G>(tw, kt, gtw, gk);
 
     TY *Y = (TY *)a.y;
+    const uint64_t pol = l2_policy_keep();
     double *ds = a.dslot + (size_t)blockIdx.x * 12 * N;
     if (!a.accumulate)
         for (int i = threadIdx.x; i < 12 * N; i += blockDim.x) ds[i] = 0.0;
     const double dt = a.dt;
     const size_t SN = (size_t)a.S * N;
 
+    constexpr int NR = (PASS == 0) ? NH - 1 : (PASS == 1 ? 1 : 0); /* history arrays read per element */
     for (int n = blockIdx.x; n < a.S; n += gridDim.x) {
         TY *yu = Y + (size_t)n * N, *yv = Y + SN + (size_t)n * N;
         const double kp2 = a.kp2[n];
+        const bool haveH = (PASS == 1) || (PASS == 3) || (PASS == 0 && !a.fk_given);
+        /* bulk L2 prefetch: this state's ABM inputs (used after the FFT phase) and the next
+         * state's y (used by the next iteration), so HBM streams while the SM computes */
+        if (threadIdx.x == 0) {
+            const size_t hb = (size_t)N * sizeof(TH), yb = (size_t)N * sizeof(TY);
+            if (PASS == 0) {
+                for (int j = 0; j < NH - 1; j++) {
+                    prefetch_l2((const TH *)a.slot[j] + (size_t)n * N, hb);
+                    prefetch_l2((const TH *)a.slot[j] + SN + (size_t)n * N, hb);
+                }
+                if (!haveH) {
+                    prefetch_l2((const TH *)a.slot[NH - 1] + (size_t)n * N, hb);
+                    prefetch_l2((const TH *)a.slot[NH - 1] + SN + (size_t)n * N, hb);
+                }
+            } else if (PASS == 1) {
+                prefetch_l2((const TH *)a.slot[NH - 2] + (size_t)n * N, hb);
+                prefetch_l2((const TH *)a.slot[NH - 2] + SN + (size_t)n * N, hb);
+            }
+            const int nn = n + gridDim.x;
+            if (nn < a.S) {
+                prefetch_l2(Y + (size_t)nn * N, yb);
+                prefetch_l2(Y + SN + (size_t)nn * N, yb);
+            }
+        }
         /* results of H land in (HU, HV) */
         C *HU = VAR ? B2 : BU, *HV = VAR ? B3 : BV;
         double E = 0.0;
-        const bool haveH = (PASS == 1) || (PASS == 0 && !a.fk_given);
         if (haveH) {
             if (VAR) E = hpsi_var<G, TY, TC>(yu, yv, BU, BV, HU, HV, tw, kt, a.cf, kp2, red);
             else E = hpsi_const<G, TY, TC>(yu, yv, BU, BV, tw, kt, a.cf, kp2, red);
             if (threadIdx.x == 0) a.qpe[n] = E;
         }
+        if (PASS == 3) {
+            for (int p = threadIdx.x; p < N; p += blockDim.x) {
+                const int o = G::off(p);
+#pragma unroll
+                for (int comp = 0; comp < 2; comp++) {
+                    const size_t gi = (comp ? SN : 0) + (size_t)n * N + p;
+                    double2 y0 = to_d(Y[gi]);
+                    C h = comp ? HV[o] : HU[o];
+                    ((TH *)a.slot[NH - 1])[gi] = from_d<TH>(make_double2((double)h.x - E * y0.x, (double)h.y - E * y0.y));
+                }
+            }
+            __syncthreads();
+            continue;
+        }
         /* ---- ABM update, unnormalised result into (HU, HV) ---- */
+        const TH *__restrict__ hs[NH];
+#pragma unroll
+        for (int j = 0; j < NH; j++) hs[j] = (const TH *)a.slot[j];
+        TH *__restrict__ fk_out = (TH *)a.slot[NH - 1];
+        TH *__restrict__ p_out = (TH *)a.slot[NH - 2];
         double nrm = 0.0;
         for (int p = threadIdx.x; p < N; p += blockDim.x) {
             const int o = G::off(p);
+            /* all global loads of this point first (both components), then arithmetic */
+            double2 y0[2], fr[2][NR > 0 ? NR : 1], fkg[2];
 #pragma unroll
             for (int comp = 0; comp < 2; comp++) {
                 const size_t gi = (comp ? SN : 0) + (size_t)n * N + p;
-                double2 y0 = to_d(Y[gi]);
+                y0[comp] = to_d(Y[gi]);
+                if (PASS == 0) {
+#pragma unroll
+                    for (int j = 0; j < NR; j++) fr[comp][j] = to_d(ld_stream(hs[j] + gi));
+                    if (!haveH) fkg[comp] = to_d(ld_stream(hs[NH - 1] + gi));
+                } else if (PASS == 1) {
+                    fr[comp][0] = to_d(ld_stream(hs[NH - 2] + gi));
+                }
+            }
+#pragma unroll
+            for (int comp = 0; comp < 2; comp++) {
+                const size_t gi = (comp ? SN : 0) + (size_t)n * N + p;
                 double2 fk = make_double2(0.0, 0.0);
-                if (PASS == 2) {
-                    /* initial measurement: normalise only (pca.c:941) */
-                } else if (haveH) {
-                    C h = comp ? HV[o] : HU[o];
-                    fk.x = (double)h.x - E * y0.x;
-                    fk.y = (double)h.y - E * y0.y;
-                } else {
-                    fk = ld2((const TH *)a.slot[NH - 1], gi);
+                if (PASS != 2) {
+                    if (haveH) {
+                        C h = comp ? HV[o] : HU[o];
+                        fk.x = (double)h.x - E * y0[comp].x;
+                        fk.y = (double)h.y - E * y0[comp].y;
+                    } else {
+                        fk = fkg[comp];
+                    }
                 }
                 double2 out;
                 if (PASS == 2) {
-                    out = y0;
+                    out = y0[comp];   /* initial measurement: normalise only (pca.c:941) */
                 } else if (PASS == 0) {
                     typedef Abm<NH> A;
                     /* sums in the reference's order: f_k*b0 - f_{k-1}*|b1| + ... */
@@ -430,18 +493,18 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
                     double2 sa = make_double2(fk.x * A::a(0), fk.y * A::a(0));
 #pragma unroll
                     for (int j = 1; j < NH; j++) {
-                        double2 fj = ld2((const TH *)a.slot[j - 1], gi);
+                        const double2 fj = fr[comp][j - 1];
                         sb.x += fj.x * A::b(j); sb.y += fj.y * A::b(j);
                         if (j < A::na) { sa.x += fj.x * A::a(j); sa.y += fj.y * A::a(j); }
                     }
                     /* y_pred = y + (-i dt) sb ; P = y + (-i dt) sa */
-                    out.x = y0.x + dt * sb.y; out.y = y0.y - dt * sb.x;
-                    double2 P = make_double2(y0.x + dt * sa.y, y0.y - dt * sa.x);
-                    if (haveH) ((TH *)a.slot[NH - 1])[gi] = from_d<TH>(fk);
-                    ((TH *)a.slot[NH - 2])[gi] = from_d<TH>(P);
+                    out.x = y0[comp].x + dt * sb.y; out.y = y0[comp].y - dt * sb.x;
+                    double2 P = make_double2(y0[comp].x + dt * sa.y, y0[comp].y - dt * sa.x);
+                    if (haveH) st_stream(fk_out + gi, from_d<TH>(fk));
+                    st_stream(p_out + gi, from_d<TH>(P));
                 } else {
                     /* y = (-i dt) f c + P */
-                    double2 P = ld2((const TH *)a.slot[NH - 2], gi);
+                    const double2 P = fr[comp][0];
                     const double c = Abm<NH>::c;
                     out.x = dt * fk.y * c + P.x;
                     out.y = -dt * fk.x * c + P.y;
@@ -460,9 +523,9 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
             double2 u = make_double2((double)hu.x * c, (double)hu.y * c);
             double2 v = make_double2((double)hv.x * c, (double)hv.y * c);
             TY su = from_d<TY>(u), sv = from_d<TY>(v);
-            yu[p] = su; yv[p] = sv;
+            st_stream(yu + p, su); st_stream(yv + p, sv);
             u = to_d(su); v = to_d(sv);
-            dens_limited(ds, p, N, u, v, f, w);
+            dens_limited(ds, p, N, u, v, f, w, pol);
             if (GRAD) {
                 C cu, cv;
                 cu.x = (TC)u.x; cu.y = (TC)u.y; cv.x = (TC)v.x; cv.y = (TC)v.y;
