@@ -46,6 +46,7 @@ struct wtd_ctx {
     size_t extra_bytes;
     int grid;
     int block;                  /* threads per CTA of the fused passes on large lattices */
+    int prefetch;               /* L2 prefetch set of the fused passes (StepArgs::prefetch) */
     int it;
     int fk_given;
     int have_coef;
@@ -124,6 +125,7 @@ static StepArgs make_args(wtd_ctx *c)
     a.cf = c->cf; a.occ = c->occ; a.kp2 = c->kp2; a.wcnt = c->wcnt;
     a.dslot = c->dslot; a.qpe = c->qpe; a.dt = c->dt; a.S = c->S;
     a.fk_given = c->fk_given;
+    a.prefetch = c->prefetch;
     a.accumulate = 0;
     return a;
 }
@@ -281,6 +283,11 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     }
     /* persistent grid: as many CTAs as fit on every SM for the most demanding pass variant
      * (the gradient pass), so all variants of a run share one slot layout */
+    c->prefetch = 3;
+    {
+        const char *pf = getenv("WTD_PREFETCH");
+        if (pf) c->prefetch = atoi(pf) & 3;
+    }
     int per_sm = occupancy_per_sm(c);
     c->grid = nsm * per_sm;
     if (c->grid > nwf) c->grid = nwf;

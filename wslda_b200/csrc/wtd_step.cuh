@@ -65,6 +65,7 @@ struct StepArgs {
     double dt;
     int S;
     int fk_given;       /* pass A: f_k is already in ring slot NH-1 */
+    int prefetch;       /* bit 0: next state's y, bit 1: this state's ABM history into L2 */
     int accumulate;     /* add to the density slot (otherwise start from zero) */
 };
 
@@ -406,7 +407,8 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
          * state's y (used by the next iteration), so HBM streams while the SM computes */
         if (threadIdx.x == 0) {
             const size_t hb = (size_t)N * sizeof(TH), yb = (size_t)N * sizeof(TY);
-            if (PASS == 0) {
+            if (!(a.prefetch & 2)) {
+            } else if (PASS == 0) {
                 for (int j = 0; j < NH - 1; j++) {
                     prefetch_l2((const TH *)a.slot[j] + (size_t)n * N, hb);
                     prefetch_l2((const TH *)a.slot[j] + SN + (size_t)n * N, hb);
@@ -420,7 +422,7 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
                 prefetch_l2((const TH *)a.slot[NH - 2] + SN + (size_t)n * N, hb);
             }
             const int nn = n + gridDim.x;
-            if (nn < a.S) {
+            if ((a.prefetch & 1) && nn < a.S) {
                 prefetch_l2(Y + (size_t)nn * N, yb);
                 prefetch_l2(Y + SN + (size_t)nn * N, yb);
             }
