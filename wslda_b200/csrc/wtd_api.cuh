@@ -283,7 +283,9 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     }
     /* persistent grid: as many CTAs as fit on every SM for the most demanding pass variant
      * (the gradient pass), so all variants of a run share one slot layout */
-    c->prefetch = 3;
+    /* L2 prefetch of the next state's y only for FP64 (prefetching the FP64 history as well
+     * overflows L2 with 148 states in flight and is re-read from HBM); FP32 forms prefetch both */
+    c->prefetch = (precision == WTD_FP64) ? 1 : 3;
     {
         const char *pf = getenv("WTD_PREFETCH");
         if (pf) c->prefetch = atoi(pf) & 3;
