@@ -84,6 +84,25 @@ int calculate_densities(int n, wtd_z *wf, wtd_z *wf_d_dx, wtd_z *wf_d_dy, wtd_z 
 int calculate_densities(int n, wtd_z *wf, wtd_z *wf_d_dx, wtd_z *d_wf_laplace, double *kkyz,
                         double *d_fbetaEn, double *weights, int *cnt, double *d_densities, int gradients_computed, int nthreads);
 #endif
+#define WTD_ERR_NOALLOC_SIZE -6
+/* calculate_densities_noalloc: no counterpart in the reference.  Same arguments, result and
+ * error behaviour as calculate_densities above, for callers that cannot call cudaMalloc (a
+ * host whose device memory is owned by a pool reserved at start-up, an embedding runtime that
+ * forbids the library from allocating): it needs no work area and allocates nothing.  Its
+ * scratch is a fixed 8 MiB device array inside the library, so it accepts lattices with
+ * 12*N doubles <= 1 Mi words (N <= 87381 points) and returns WTD_ERR_NOALLOC_SIZE (-6)
+ * otherwise.  The array is shared by all calls: calls that overlap on the GPU race on it.
+ * The first call on a device resolves the array's device address with that device current. */
+#if WTD_CODEDIM == 3
+int calculate_densities_noalloc(int n, wtd_z *wf, wtd_z *wf_d_dx, wtd_z *wf_d_dy, wtd_z *wf_d_dz, wtd_z *d_wf_laplace,
+                                double *d_fbetaEn, double *weights, double *d_densities, int gradients_computed, int nthreads);
+#elif WTD_CODEDIM == 2
+int calculate_densities_noalloc(int n, wtd_z *wf, wtd_z *wf_d_dx, wtd_z *wf_d_dy, wtd_z *d_wf_laplace, double *kkz,
+                                double *d_fbetaEn, double *weights, double *d_densities, int gradients_computed, int nthreads);
+#else
+int calculate_densities_noalloc(int n, wtd_z *wf, wtd_z *wf_d_dx, wtd_z *d_wf_laplace, double *kkyz,
+                                double *d_fbetaEn, double *weights, int *cnt, double *d_densities, int gradients_computed, int nthreads);
+#endif
 int density_caculate_tau(double *d_densities, int nthreads);
 int symmetrize_densities_device(double *d_densities);
 

@@ -259,6 +259,7 @@ const char *wtd_error_string(int code)
     case WTD_ERR_UNSUPPORTED: return "lattice/mode not supported by this build";
     case WTD_ERR_STATE: return "call out of order";
     case WTD_ERR_NOMEM: return "out of device memory";
+    case -6: return "lattice too large for the fixed scratch of calculate_densities_noalloc (12*N doubles > 1 Mi words)";
     default: return "unknown error";
     }
 }

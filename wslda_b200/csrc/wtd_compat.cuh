@@ -407,6 +407,113 @@ static int compat_planewave(int n, const double *kky, const double *kkz, const i
 }
 
 /* ---------------------------------------------------------------------------------------
+ * calculate_densities without any allocation
+ *
+ * Some callers cannot call cudaMalloc: hosts whose device memory is owned by another
+ * allocator (a pool reserved once at start-up, as the reference's driver sizes every device
+ * buffer up front at pca.c:749-765 and treats any later allocation as fatal) and embedding
+ * runtimes that forbid a library from allocating device memory on their behalf.  For them
+ * calculate_densities_noalloc computes the same densities as calculate_densities without a
+ * work area: the per-CTA FP64 partial sums live in the file-scope array below, which every
+ * GPU that loads this library holds until the process exits.
+ *
+ * Limit: WTD_NOALLOC_BYTES (8 MiB) of scratch, i.e. lattices with 12*N doubles <= 1 Mi words
+ * (N <= 87381 points); larger lattices are rejected with WTD_ERR_NOALLOC_SIZE before any
+ * work is issued.  The number of CTAs is min(2 per SM, n, 8 MiB / (12*N*8)).
+ * Every call shares the array and leaves its partial sums in it; each call clears the part it
+ * uses first.  Calls that overlap on the GPU (other host threads, other streams) race on it.
+ * -------------------------------------------------------------------------------------*/
+#define WTD_NOALLOC_BYTES (8u << 20)
+static __device__ __align__(256) double wtd_noalloc_scratch[WTD_NOALLOC_BYTES / sizeof(double)];
+static double *g_noalloc_scratch[64];   /* device address of wtd_noalloc_scratch, per device */
+
+/* the array's name is a host-side stand-in, not a device address: resolve it once per
+ * device, with that device current, and pass the resolved pointer to the kernels */
+static int noalloc_scratch(double **out)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return WTD_ERR_CUDA;
+    if (dev < 0 || dev >= 64) return WTD_ERR_ARG;
+    if (!g_noalloc_scratch[dev]) {
+        double *p = NULL;
+        if (cudaGetSymbolAddress((void **)&p, wtd_noalloc_scratch) != cudaSuccess || !p) return WTD_ERR_CUDA;
+        g_noalloc_scratch[dev] = p;
+    }
+    *out = g_noalloc_scratch[dev];
+    return WTD_OK;
+}
+
+/* k_dens_compat with the per-state plane-wave weights formed in the kernel (so no per-state
+ * arrays are needed) */
+__global__ void k_dens_noalloc(int n, const double2 *wf, const double2 *dx, const double2 *dy, const double2 *dz,
+                               const double2 *lap, const double *fb, const double *wts, const double *kky,
+                               const double *kkz, const int *cnt, double *slots, int grads)
+{
+    constexpr int N = WTD_NUMEL;
+    double *ds = slots + (size_t)blockIdx.x * 12 * N;
+    const uint64_t pol = l2_policy_keep();
+    for (int i = threadIdx.x; i < 12 * N; i += blockDim.x) ds[i] = 0.0;
+    __syncthreads();
+    const size_t SN = (size_t)n * N;
+    for (int s = blockIdx.x; s < n; s += gridDim.x) {
+        double ky = kky ? kky[s] : 0.0, kz = kkz ? kkz[s] : 0.0, k2 = 0.0, wc = 1.0;
+#if CODEDIM == 2
+        k2 = kz * kz;
+        wc = (fabs(kz) < 1.0e-12) ? 1.0 : 2.0;
+#ifdef USE_CUBIC_CUTOFF
+        if (fabs(kz + M_PI / DZ) < 1.0e-12) wc = 1.0;
+#endif
+#elif CODEDIM == 1
+        k2 = ky * ky + kz * kz;
+        wc = cnt ? (double)cnt[s] : 1.0;
+#endif
+        (void)ky; (void)kz;
+        const double f = fb[s];
+        const double w = (wts ? wts[s] : 1.0) * wc;
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            const size_t iu = (size_t)s * N + p, iv = SN + iu;
+            double2 u = wf[iu], v = wf[iv];
+            dens_limited(ds, p, N, u, v, f, w, pol);
+            if (grads) {
+                const double fa = f * w, fbm = (1.0 - f) * w;
+                double2 lu = lap[iu], lv = lap[iv];
+                ds[3 * (size_t)N + p] += (u.x * (lu.x - u.x * k2) + u.y * (lu.y - u.y * k2)) * fa;
+                ds[8 * (size_t)N + p] += (v.x * (lv.x - v.x * k2) + v.y * (lv.y - v.y * k2)) * fbm;
+                const double2 *dd[3] = {dx, dy, dz};
+                for (int d = 0; d < CODEDIM; d++) {
+                    double2 a = dd[d][iu], b = dd[d][iv];
+                    ds[(4 + d) * (size_t)N + p] += (u.x * a.y - u.y * a.x) * fa;
+                    ds[(9 + d) * (size_t)N + p] -= (v.x * b.y - v.y * b.x) * fbm;
+                }
+            }
+        }
+    }
+}
+
+static int calculate_densities_noalloc_impl(int n, wtd_z *wf, wtd_z *dx, wtd_z *dy, wtd_z *dz, wtd_z *lap,
+                                            const double *kky, const double *kkz, const int *cnt, double *fb,
+                                            double *w, double *dens, int grads)
+{
+    const size_t per_cta = (size_t)12 * WTD_NUMEL;
+    const size_t cap = WTD_NOALLOC_BYTES / sizeof(double);
+    if (per_cta > cap) return WTD_ERR_NOALLOC_SIZE;
+    if (n <= 0 || !wf || !fb || !dens || (grads && !lap)) return WTD_ERR_ARG;
+    double *slots = NULL;
+    int r = noalloc_scratch(&slots);
+    if (r) return r;
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    int G = 2 * nsm;
+    if (G > n) G = n;
+    if ((size_t)G > cap / per_cta) G = (int)(cap / per_cta);
+    k_dens_noalloc<<<G, 256>>>(n, (const double2 *)wf, (const double2 *)dx, (const double2 *)dy, (const double2 *)dz,
+                               (const double2 *)lap, fb, w, kky, kkz, cnt, slots, grads);
+    wtd_dens_reduce<<<(12 * WTD_NUMEL + 255) / 256, 256>>>(slots, G, dens, WTD_NUMEL, grads ? 1 : 0, 1.0 / WTD_LPERP);
+    return cu_sync_status();
+}
+
+/* ---------------------------------------------------------------------------------------
  * entry points
  * -------------------------------------------------------------------------------------*/
 extern "C" {
@@ -585,6 +692,26 @@ int calculate_densities(int n, wtd_z *wf, wtd_z *dx, wtd_z *dy, wtd_z *lap, doub
 int calculate_densities(int n, wtd_z *wf, wtd_z *dx, wtd_z *lap, double *kkyz, double *fb, double *w, int *cnt, double *dens, int grads, int nthreads)
 {
     return calculate_densities_impl(n, wf, dx, NULL, NULL, lap, kkyz, kkyz ? kkyz + n : NULL, cnt, fb, w, dens, grads);
+}
+#endif
+
+#if CODEDIM == 3
+int calculate_densities_noalloc(int n, wtd_z *wf, wtd_z *dx, wtd_z *dy, wtd_z *dz, wtd_z *lap, double *fb, double *w,
+                                double *dens, int grads, int nthreads)
+{
+    return calculate_densities_noalloc_impl(n, wf, dx, dy, dz, lap, NULL, NULL, NULL, fb, w, dens, grads);
+}
+#elif CODEDIM == 2
+int calculate_densities_noalloc(int n, wtd_z *wf, wtd_z *dx, wtd_z *dy, wtd_z *lap, double *kkz, double *fb, double *w,
+                                double *dens, int grads, int nthreads)
+{
+    return calculate_densities_noalloc_impl(n, wf, dx, dy, NULL, lap, NULL, kkz, NULL, fb, w, dens, grads);
+}
+#else
+int calculate_densities_noalloc(int n, wtd_z *wf, wtd_z *dx, wtd_z *lap, double *kkyz, double *fb, double *w, int *cnt,
+                                double *dens, int grads, int nthreads)
+{
+    return calculate_densities_noalloc_impl(n, wf, dx, NULL, NULL, lap, kkyz, kkyz ? kkyz + n : NULL, cnt, fb, w, dens, grads);
 }
 #endif
 
