@@ -53,3 +53,15 @@ def test_c2_slda2d_small_s(has_gpu):
 @pytest.mark.gpu
 def test_c4_bdg2d_small_s(has_gpu):
     _compare("c4_bdg2d", nwf=32, nsteps=4, nmeas=1)
+
+
+@pytest.mark.gpu
+def test_c3_aslda3d_small_s(has_gpu):
+    """3D ASLDA 32^3 (state larger than one CTA): the staged plane/pencil path."""
+    _compare("c3_aslda3d", nwf=8, nsteps=2, nmeas=1)
+
+
+@pytest.mark.gpu
+def test_c5_slda3d_small_s(has_gpu):
+    """3D SLDA 48^3 (radix-3 axes) through the staged path."""
+    _compare("c5_slda3d", nwf=4, nsteps=2, nmeas=1)

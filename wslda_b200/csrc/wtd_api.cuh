@@ -12,25 +12,7 @@
 #ifndef WTD_API_CUH
 #define WTD_API_CUH
 
-#include <stdlib.h>
-#include <string.h>
-#include <math.h>
-#include "wtd.h"
-#include "wtd_aux.cuh"
-
-#if CODEDIM == 1
-typedef Geo<NX, 1, 1> WG;
-#elif CODEDIM == 2
-typedef Geo<NX, NY, 1> WG;
-#else
-typedef Geo<NX, NY, NZ> WG;
-#endif
-
-#ifdef FAST_CONST_EFFECTIVE_MASS_MODE
-#define WTD_VAR false
-#else
-#define WTD_VAR true
-#endif
+#include "wtd_lattice.cuh"
 
 struct wtd_ctx {
     int dev, S, prec;
@@ -57,11 +39,11 @@ struct wtd_ctx {
     int timing;
     cudaEvent_t ev[2][2][4096];
     int nev[2];
+    /* large 3D lattices (state larger than one CTA's shared memory): staged path */
+    int staged;
+    double2 *ddx, *ddy, *ddz, *dlap, *dalap, *stage3d;
 };
 
-static int wtd_cuerr(cudaError_t e) { return e == cudaSuccess ? WTD_OK : WTD_ERR_CUDA; }
-#define WTD_TRY(x) do { int _r = (x); if (_r) return _r; } while (0)
-#define WTD_CU(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return WTD_ERR_CUDA; } while (0)
 #define WTD_LAUNCHED(ctx) do { (ctx)->launches++; cudaError_t _e = cudaGetLastError(); if (_e != cudaSuccess) return WTD_ERR_CUDA; } while (0)
 
 static size_t elem_bytes_y(int prec) { return prec == WTD_FP64 ? sizeof(double2) : sizeof(float2); }
@@ -71,7 +53,6 @@ static size_t elem_bytes_h(int prec) { return prec == WTD_MIXED_H32 ? sizeof(flo
  * fused pass dispatch
  * -------------------------------------------------------------------------------------*/
 template <typename TC, int NBUF> static constexpr size_t fused_smem() { return FusedSmem<WG, TC, NBUF>::bytes; }
-static constexpr size_t WTD_SMEM_MAX = 232448;
 
 template <typename TY, typename TH, typename TC, int PASS, bool GRAD>
 static int launch_pass_t(wtd_ctx *c, StepArgs &a)
@@ -199,6 +180,114 @@ static int after_pass(wtd_ctx *c, bool full, int it)
     return WTD_OK;
 }
 
+/* ---------------------------------------------------------------------------------------
+ * staged step for lattices whose state does not fit one CTA (32^3, 48^3): the reference's
+ * per-step sequence (pca.c:1401-1571) on this library's kernels — plane/pencil spectral
+ * derivatives (wtd_fft3d.cuh), CTA-per-state renormalisation and H psi with <H> subtraction,
+ * slot-accumulated densities, the ABM update as one elementwise kernel per half step.
+ * -------------------------------------------------------------------------------------*/
+static int staged_densities(wtd_ctx *c, bool grads)
+{
+    constexpr int N = WTD_NUMEL;
+    const int S = c->S;
+    int G = c->grid;
+    k_dens_compat<<<G, 256, 0, c->st>>>(S, (const double2 *)c->y, c->ddx, c->ddy, c->ddz, c->dlap, c->occ, NULL, c->kp2,
+                                        c->wcnt, c->dslot, grads ? 1 : 0);
+    WTD_LAUNCHED(c);
+    wtd_dens_reduce<<<(12 * N + 255) / 256, 256, 0, c->st>>>(c->dslot, G, c->dens, N, grads ? 1 : 0, 1.0 / WTD_LPERP);
+    WTD_LAUNCHED(c);
+    if (grads) WTD_TRY(big_tau(c->dens, c->stage3d, c->tw, c->ktab, c->st));
+    return WTD_OK;
+}
+
+static int staged_derivs(wtd_ctx *c, bool grads)
+{
+    const int nf = 2 * c->S;
+    if (grads) return big_derivs((double2 *)c->y, nf, c->dlap, c->ddx, c->ddy, c->ddz, c->tw, c->ktab, c->st);
+    return big_derivs((double2 *)c->y, nf, c->dlap, NULL, NULL, NULL, c->tw, c->ktab, c->st);
+}
+
+static int staged_potentials(wtd_ctx *c, int it)
+{
+    constexpr int N = WTD_NUMEL;
+    wslda_density D = convert_into_wslda_density(c->dens, N);
+    wslda_potential P = convert_into_wslda_potential(c->pots, N, NULL);
+    int pb = (N + 127) / 128;
+    wtd_potentials_kernel<<<pb, 128, 0, c->st>>>(it, D, P, 1.0);
+    WTD_LAUNCHED(c);
+#ifdef ENABLE_MODIFY_POTENTIALS
+    modify_potentials<<<pb, 128, 0, c->st>>>(it, D, P);
+    WTD_LAUNCHED(c);
+#endif
+    wtd_prep_coef<<<pb, 128, 0, c->st>>>(it, P, c->cf);
+    WTD_LAUNCHED(c);
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+    WTD_TRY(big_prep_var(c->cf, c->stage3d, c->tw, c->ktab, c->st));
+    /* lap(alpha psi) for the variable-mass kinetic term (pca.c:1455-1456) */
+    size_t M = (size_t)2 * c->S * N;
+    k_mul_alpha<<<(unsigned)((M + 255) / 256), 256, 0, c->st>>>(c->S, (const double2 *)c->y, c->dalap, P.alpha_a, P.alpha_b);
+    WTD_LAUNCHED(c);
+    WTD_TRY(big_derivs(c->dalap, 2 * c->S, c->dalap, NULL, NULL, NULL, c->tw, c->ktab, c->st));
+#endif
+    c->have_coef = 1;
+    return WTD_OK;
+}
+
+static int staged_hamiltonian(wtd_ctx *c, double2 *out)
+{
+    k_hamiltonian_compat<<<c->S, 256, 0, c->st>>>(c->S, (const double2 *)c->y, out, c->ddx, c->ddy, c->ddz, c->dlap,
+                                                  c->dalap, c->cf, c->kp2, c->qpe, NULL);
+    WTD_LAUNCHED(c);
+    return WTD_OK;
+}
+
+static int staged_initial(wtd_ctx *c)
+{
+    k_normalize<<<c->S, 256, 0, c->st>>>(c->S, (double2 *)c->y);
+    WTD_LAUNCHED(c);
+    WTD_TRY(staged_derivs(c, true));
+    return staged_densities(c, true);
+}
+
+static int staged_step(wtd_ctx *c, bool last)
+{
+    constexpr int N = WTD_NUMEL;
+    const int NH = WTD_NHIST;
+    const size_t M = (size_t)2 * c->S * N;
+    const unsigned nb = (unsigned)((M + 255) / 256);
+    /* the reference's f1..fq from the ring (f1 newest at ring position NH-1) */
+    double2 *f[5] = {NULL, NULL, NULL, NULL, NULL};
+    for (int sl = 0; sl < NH; sl++) f[sl] = (double2 *)c->hist[(c->head + (sl == 0 ? NH - 1 : sl - 1)) % NH];
+    const bool var = WTD_VAR;
+    /* predictor (pca.c:1407-1465) */
+    if (NH == 3) k_abm_step1<3><<<nb, 256, 0, c->st>>>(M, (double2 *)c->y, f[0], f[1], f[2], NULL, NULL, c->dt);
+    else if (NH == 4) k_abm_step1<4><<<nb, 256, 0, c->st>>>(M, (double2 *)c->y, f[0], f[1], f[2], f[3], NULL, c->dt);
+    else k_abm_step1<5><<<nb, 256, 0, c->st>>>(M, (double2 *)c->y, f[0], f[1], f[2], f[3], f[4], c->dt);
+    WTD_LAUNCHED(c);
+    k_normalize<<<c->S, 256, 0, c->st>>>(c->S, (double2 *)c->y);
+    WTD_LAUNCHED(c);
+    WTD_TRY(staged_derivs(c, var));
+    WTD_TRY(staged_densities(c, var));
+    WTD_TRY(staged_potentials(c, c->it + 1));
+    WTD_TRY(staged_hamiltonian(c, c->dlap));
+    /* corrector (pca.c:1469-1566) */
+    const double cc = (NH == 3) ? 9. / 24. : 251. / 720.;
+    k_abm_step4<<<nb, 256, 0, c->st>>>(M, c->dlap, (double2 *)c->y, f[NH - 1], c->dt, cc);
+    WTD_LAUNCHED(c);
+    k_normalize<<<c->S, 256, 0, c->st>>>(c->S, (double2 *)c->y);
+    WTD_LAUNCHED(c);
+    const bool g = var || last;
+    WTD_TRY(staged_derivs(c, g));
+    WTD_TRY(staged_densities(c, g));
+    WTD_TRY(staged_potentials(c, c->it + 1));
+    /* pointer rotation (pca.c:1543-1562): the old f_q slot (P, consumed) becomes f1 */
+    WTD_TRY(staged_hamiltonian(c, f[NH - 1]));
+    c->head = (c->head + NH - 1) % NH;
+    c->fk_given = 1;
+    c->it++;
+    return WTD_OK;
+}
+
 template <typename TY, typename TH, typename TC>
 static int occupancy_t(int block)
 {
@@ -246,8 +335,10 @@ int wtd_info(int *dims, int *numel, int *codedim, int *nhist, int *functional, i
 size_t wtd_device_bytes(int nwf, int precision)
 {
     size_t n2 = (size_t)2 * nwf * WTD_NUMEL;
-    return n2 * (elem_bytes_y(precision) + WTD_NHIST * elem_bytes_h(precision)) +
-           (size_t)160 * 12 * WTD_NUMEL * sizeof(double);
+    size_t b = n2 * (elem_bytes_y(precision) + WTD_NHIST * elem_bytes_h(precision)) +
+               (size_t)300 * 12 * WTD_NUMEL * sizeof(double);
+    if (WTD_BIG) b += n2 * sizeof(double2) * (WTD_VAR ? 5 : 4);
+    return b;
 }
 
 const char *wtd_error_string(int code)
@@ -291,7 +382,9 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
         const char *pf = getenv("WTD_PREFETCH");
         if (pf) c->prefetch = atoi(pf) & 3;
     }
-    int per_sm = occupancy_per_sm(c);
+    c->staged = WTD_BIG ? 1 : 0;
+    if (c->staged && precision != WTD_FP64) { free(c); return WTD_ERR_UNSUPPORTED; }
+    int per_sm = c->staged ? 2 : occupancy_per_sm(c);
     c->grid = nsm * per_sm;
     if (c->grid > nwf) c->grid = nwf;
     cudaError_t e = cudaSuccess;
@@ -311,33 +404,27 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     ALLOC(c->tw, WG::twtotal * sizeof(double2));
     ALLOC(c->ktab, 6 * 128 * sizeof(double));
     if (precision != WTD_FP64) ALLOC(c->stage, n2 * sizeof(double2));
+    if (c->staged) {
+        ALLOC(c->ddx, n2 * sizeof(double2));
+        ALLOC(c->ddy, n2 * sizeof(double2));
+        ALLOC(c->ddz, n2 * sizeof(double2));
+        ALLOC(c->dlap, n2 * sizeof(double2));
+        if (WTD_VAR) ALLOC(c->dalap, n2 * sizeof(double2));
+        ALLOC(c->stage3d, 2 * N * sizeof(double2));
+    }
 #undef ALLOC
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
     if (e != cudaSuccess) { wtd_destroy(c); return e == cudaErrorMemoryAllocation ? WTD_ERR_NOMEM : WTD_ERR_CUDA; }
     cudaMemsetAsync(c->cf, 0, (size_t)CF_COUNT * N * sizeof(double), c->st);
     cudaMemsetAsync(c->qpe, 0, nwf * sizeof(double), c->st);
     cudaMemsetAsync(c->dens, 0, 12 * N * sizeof(double), c->st);
-    /* FFT twiddles e^{-2 pi i t/n} and wave-number tables of digit-reversed positions */
     {
         double2 tw[WG::twtotal];
         double kt[6 * 128];
-        memset(kt, 0, sizeof(kt));
-        const double Lax[3] = {LX, LY, LZ};
-        for (int a = 0; a < 3; a++) {
-            int n = WG::n(a);
-            for (int t = 0; t < n; t++) {
-                long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)t / (long double)n;
-                tw[WG::twoff(a) + t] = make_double2((double)cosl(ang), -(double)sinl(ang));
-            }
-            for (int p = 0; p < n && p < 128; p++) {
-                int f = dif_freq(n, p);
-                double k = (f < n / 2) ? 2. * M_PI / Lax[a] * (double)f : 2. * M_PI / Lax[a] * (double)(f - n);
-                kt[a * 128 + p] = (n > 1) ? k : 0.0;
-                kt[(3 + a) * 128 + p] = (n > 1 && f != n / 2) ? k : 0.0;
-            }
-        }
+        wtd_make_tables(tw, kt);
         cudaMemcpyAsync(c->tw, tw, sizeof(tw), cudaMemcpyHostToDevice, c->st);
         cudaMemcpyAsync(c->ktab, kt, sizeof(kt), cudaMemcpyHostToDevice, c->st);
+        cudaStreamSynchronize(c->st);
     }
     /* defaults: f_n = 0, no plane-wave momentum, unit degeneracy */
     {
@@ -366,7 +453,7 @@ int wtd_destroy(wtd_ctx *c)
             for (int k = 0; k < 2; k++)
                 for (int i = 0; i < 4096; i++) cudaEventDestroy(c->ev[p][k][i]);
     void *ptrs[] = {c->y, c->cf, c->occ, c->kp2, c->wcnt, c->dslot, c->qpe, c->dens, c->pots, c->ework,
-                    c->eout, c->tw, c->ktab, c->stage, c->extra};
+                    c->eout, c->tw, c->ktab, c->stage, c->extra, c->ddx, c->ddy, c->ddz, c->dlap, c->dalap, c->stage3d};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) if (ptrs[i]) cudaFree(ptrs[i]);
     for (int h = 0; h < WTD_NHIST; h++) if (c->hist[h]) cudaFree(c->hist[h]);
     if (c->st) cudaStreamDestroy(c->st);
@@ -545,6 +632,10 @@ int wtd_initial_measurement(wtd_ctx *c, int it0)
     c->head = 0;
     for (int h = 0; h < WTD_NHIST; h++) WTD_CU(cudaMemsetAsync(c->hist[h], 0, c->hsz, c->st));
     c->fk_given = 1;
+    if (c->staged) {
+        WTD_TRY(staged_initial(c));
+        return wtd_cuerr(cudaGetLastError());
+    }
     WTD_TRY(run_pass(c, 2, true));
     WTD_TRY(after_pass(c, true, -1));
     return wtd_cuerr(cudaGetLastError());
@@ -555,6 +646,10 @@ int wtd_steps(wtd_ctx *c, int nsteps)
     if (!c || nsteps < 0) return WTD_ERR_ARG;
     WTD_CU(cudaSetDevice(c->dev));
     const bool var = WTD_VAR;
+    if (c->staged) {
+        for (int s = 0; s < nsteps; s++) WTD_TRY(staged_step(c, s == nsteps - 1));
+        return WTD_OK;
+    }
     for (int s = 0; s < nsteps; s++) {
         const bool last = (s == nsteps - 1);
         if (!c->fk_given && !c->have_coef) return WTD_ERR_STATE;

@@ -318,21 +318,7 @@ static int compat_tables(void)
     if (g_tw) return 0;
     double2 tw[WG::twtotal];
     double kt[6 * 128];
-    memset(kt, 0, sizeof(kt));
-    const double Lax[3] = {LX, LY, LZ};
-    for (int a = 0; a < 3; a++) {
-        int n = WG::n(a);
-        for (int t = 0; t < n; t++) {
-            long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)t / (long double)n;
-            tw[WG::twoff(a) + t] = make_double2((double)cosl(ang), -(double)sinl(ang));
-        }
-        for (int p = 0; p < n && p < 128; p++) {
-            int f = dif_freq(n, p);
-            double k = (f < n / 2) ? 2. * M_PI / Lax[a] * (double)f : 2. * M_PI / Lax[a] * (double)(f - n);
-            kt[a * 128 + p] = (n > 1) ? k : 0.0;
-            kt[(3 + a) * 128 + p] = (n > 1 && f != n / 2) ? k : 0.0;
-        }
-    }
+    wtd_make_tables(tw, kt);
     if (cudaMalloc((void **)&g_tw, sizeof(tw)) != cudaSuccess) return WTD_ERR_NOMEM;
     if (cudaMalloc((void **)&g_ktab, sizeof(kt)) != cudaSuccess) return WTD_ERR_NOMEM;
     cudaMemcpy(g_tw, tw, sizeof(tw), cudaMemcpyHostToDevice);
@@ -340,11 +326,22 @@ static int compat_tables(void)
     return 0;
 }
 
-static constexpr size_t k_derivs_smem = 2 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
-static constexpr size_t k_field_smem = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
+
+static double2 *g_stage3d = NULL;
+static int compat_stage(void)
+{
+    if (g_stage3d) return 0;
+    return cudaMalloc((void **)&g_stage3d, 2 * sizeof(double2) * WTD_NUMEL) == cudaSuccess ? 0 : WTD_ERR_NOMEM;
+}
 
 static int compat_real_deriv(const double *f, double *out, int which)
 {
+    if (WTD_BIG) {
+        WTD_TRY(compat_tables());
+        WTD_TRY(compat_stage());
+        WTD_TRY(big_real_deriv(f, out, which, 1.0, 0, g_stage3d, g_tw, g_ktab, 0));
+        return cu_sync_status();
+    }
     if (k_field_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     int r = compat_tables();
     if (r) return r;
@@ -360,11 +357,16 @@ static int compat_coefficients(int it, double *pots)
     double *cf = compat_cf();
     wtd_prep_coef<<<(WTD_NUMEL + 127) / 128, 128>>>(it, P, cf);
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
-    if (k_field_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     int r = compat_tables();
     if (r) return r;
-    cudaFuncSetAttribute(wtd_prep_var<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k_field_smem);
-    wtd_prep_var<WG><<<2, 256, k_field_smem>>>(cf, g_tw, g_ktab);
+    if (WTD_BIG) {
+        WTD_TRY(compat_stage());
+        WTD_TRY(big_prep_var(cf, g_stage3d, g_tw, g_ktab, 0));
+    } else {
+        if (k_field_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+        cudaFuncSetAttribute(wtd_prep_var<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k_field_smem);
+        wtd_prep_var<WG><<<2, 256, k_field_smem>>>(cf, g_tw, g_ktab);
+    }
 #endif
     return cu_sync_status();
 }
@@ -614,9 +616,13 @@ int normalize_wf(int n, wtd_z *wf, int nthreads)
 }
 int compute_derivatives(int n, wtd_z *wf, wtd_z *dx, wtd_z *dy, wtd_z *dz, wtd_z *lap, int nthreads)
 {
-    if (k_derivs_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     int r = compat_tables();
     if (r) return r;
+    if (WTD_BIG) {
+        WTD_TRY(big_derivs((double2 *)wf, n, (double2 *)lap, (double2 *)dx, (double2 *)dy, (double2 *)dz, g_tw, g_ktab, 0));
+        return cu_sync_status();
+    }
+    if (k_derivs_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     cudaFuncSetAttribute(k_derivs<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k_derivs_smem);
     k_derivs<WG><<<n, 512, k_derivs_smem>>>((const double2 *)wf, (double2 *)dx, CODEDIM >= 2 ? (double2 *)dy : NULL,
                                              CODEDIM >= 3 ? (double2 *)dz : NULL, (double2 *)lap, g_tw, g_ktab);
@@ -624,9 +630,13 @@ int compute_derivatives(int n, wtd_z *wf, wtd_z *dx, wtd_z *dy, wtd_z *dz, wtd_z
 }
 int compute_laplace(int n, wtd_z *wf, wtd_z *lap, int nthreads)
 {
-    if (k_derivs_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     int r = compat_tables();
     if (r) return r;
+    if (WTD_BIG) {
+        WTD_TRY(big_derivs((double2 *)wf, n, (double2 *)lap, NULL, NULL, NULL, g_tw, g_ktab, 0));
+        return cu_sync_status();
+    }
+    if (k_derivs_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     cudaFuncSetAttribute(k_derivs<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k_derivs_smem);
     k_derivs<WG><<<n, 512, k_derivs_smem>>>((const double2 *)wf, NULL, NULL, NULL, (double2 *)lap, g_tw, g_ktab);
     return cu_sync_status();
@@ -717,9 +727,14 @@ int calculate_densities_noalloc(int n, wtd_z *wf, wtd_z *dx, wtd_z *lap, double 
 
 int density_caculate_tau(double *dens, int nthreads)
 {
-    if (k_field_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     int r = compat_tables();
     if (r) return r;
+    if (WTD_BIG) {
+        WTD_TRY(compat_stage());
+        WTD_TRY(big_tau(dens, g_stage3d, g_tw, g_ktab, 0));
+        return cu_sync_status();
+    }
+    if (k_field_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     cudaFuncSetAttribute(wtd_tau_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k_field_smem);
     wtd_tau_kernel<WG><<<2, 512, k_field_smem>>>(dens, g_tw, g_ktab);
     return cu_sync_status();

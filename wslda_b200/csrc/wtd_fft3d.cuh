@@ -1,0 +1,200 @@
+/*
+ * Spectral derivatives of 3D fields too large for one CTA's shared memory (32^3, 48^3 ...):
+ * a plane/pencil decomposition through global memory.
+ *
+ *   k_planes  : one CTA per (field, x-plane) — 2D FFT over (y, z) of a contiguous plane in smem
+ *   k_pencils : one CTA per (field, group of PX consecutive (y, z) pencils) — FFT along x,
+ *               then for every requested operator: multiply by -|k|^2/N or i k_d/N (Nyquist
+ *               zeroed for first derivatives, pca_derivative.cu:152-171), inverse FFT along x,
+ *               store.  The (y, z) wave numbers come from the digit-reversed plane positions.
+ *   inverse planes on every output.
+ *
+ * A derivative set of nf fields costs 1 + nops + 2*nops array passes of reads and writes
+ * (laplacian only: 3 reads + 3 writes), against the reference's cuFFT forward, multiply
+ * kernel and one cuFFT inverse per output (pca_derivative.cu:217-277).
+ */
+#ifndef WTD_FFT3D_CUH
+#define WTD_FFT3D_CUH
+
+#include "wtd_step.cuh"
+
+#define WTD_PX 16   /* pencils per CTA */
+
+/* 2D (y, z) transform of plane x of field f: in -> out (may alias), fields of N points each */
+template <class GP, int SIGN>
+__global__ void __launch_bounds__(512) k_planes(const double2 *in, double2 *out, int nx, const double2 *gtw_yz, const double *gk)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *B = (double2 *)smem_raw;
+    double2 *tw = B + GP::padded;
+    double (*kt)[128] = (double (*)[128])(tw + GP::twtotal);
+    (void)kt;
+    (void)nx;
+    for (int t = threadIdx.x; t < GP::N0 + GP::N1; t += blockDim.x) tw[t] = gtw_yz[t];
+    constexpr int NP = GP::ntot;
+    const size_t base = (size_t)blockIdx.x * NP;   /* blockIdx.x = f * nx + x: planes are contiguous */
+    for (int p = threadIdx.x; p < NP; p += blockDim.x) B[GP::off(p)] = in[base + p];
+    __syncthreads();
+    if (SIGN < 0) fft_forward<GP, 1>(B, 0, tw);
+    else fft_inverse<GP, 1>(B, 0, tw);
+    for (int p = threadIdx.x; p < NP; p += blockDim.x) out[base + p] = B[GP::off(p)];
+}
+
+/* x-pencil pass: forward x FFT, then per operator multiply + inverse x FFT.
+ * in: fields already (y, z)-transformed; out[op] gets op applied (still (y, z)-transformed).
+ * ops bit 0: laplacian, bit 1..3: d/dx, d/dy, d/dz.  Outputs may alias the input. */
+template <class GX>
+__global__ void __launch_bounds__(512) k_pencils(const double2 *in, double2 *olap, double2 *odx, double2 *ody, double2 *odz,
+                                                 int nyz, int N, const double2 *gtw_x, const double *gk)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *B0 = (double2 *)smem_raw;
+    double2 *W = B0 + GX::padded;
+    double2 *tw = W + GX::padded;
+    double (*kt)[128] = (double (*)[128])(tw + GX::twtotal);
+    constexpr int NXL = GX::N0, PX = GX::N1;
+    for (int t = threadIdx.x; t < NXL; t += blockDim.x) tw[t] = gtw_x[t];
+    for (int t = threadIdx.x; t < 6 * 128; t += blockDim.x) kt[t / 128][t % 128] = gk[t];
+    const int groups = nyz / PX;
+    const int f = blockIdx.x / groups, g = blockIdx.x - f * groups;
+    const size_t fb = (size_t)f * N;
+    const int q0 = g * PX;
+    /* element (x, q) of the field sits at x*nyz + q */
+    for (int i = threadIdx.x; i < NXL * PX; i += blockDim.x) {
+        int x = i / PX, j = i - x * PX;
+        B0[GX::off(x * PX + j)] = in[fb + (size_t)x * nyz + q0 + j];
+    }
+    __syncthreads();
+    fft_axis_fwd<GX, 0, 0, NXL, 1>(B0, 0, tw);
+    double2 *outs[4] = {olap, odx, ody, odz};
+    for (int op = 0; op < 4; op++) {
+        double2 *o = outs[op];
+        if (!o) continue;
+        for (int i = threadIdx.x; i < NXL * PX; i += blockDim.x) {
+            int x = i / PX, j = i - x * PX;
+            int q = q0 + j;
+            int yq = q / NZ, zq = q - yq * NZ;
+            double2 z = B0[GX::off(x * PX + j)];
+            double2 r;
+            if (op == 0) {
+                double kx = kt[0][x], ky = kt[1][yq], kz = kt[2][zq];
+                double s = -1.0 * (kx * kx + ky * ky + kz * kz) / (double)N;
+                r = make_double2(z.x * s, z.y * s);
+            } else {
+                double k = (op == 1) ? kt[3][x] : (op == 2) ? kt[4][yq] : kt[5][zq];
+                double s = k / (double)N;
+                r = make_double2(-s * z.y, s * z.x);
+            }
+            W[GX::off(x * PX + j)] = r;
+        }
+        __syncthreads();
+        fft_axis_inv<GX, 0, NXL, 1>(W, 0, tw);
+        for (int i = threadIdx.x; i < NXL * PX; i += blockDim.x) {
+            int x = i / PX, j = i - x * PX;
+            o[fb + (size_t)x * nyz + q0 + j] = W[GX::off(x * PX + j)];
+        }
+        __syncthreads();
+    }
+}
+
+typedef Geo<NY, NZ, 1> WGP;          /* one (y, z) plane */
+typedef Geo<NX, WTD_PX, 1> WGX;      /* PX pencils along x */
+
+static constexpr size_t planes_smem = (size_t)WGP::padded * sizeof(double2) + WGP::twtotal * sizeof(double2) + sizeof(KTab<WGP>);
+static constexpr size_t pencils_smem = 2 * (size_t)WGX::padded * sizeof(double2) + WGX::twtotal * sizeof(double2) + sizeof(KTab<WGX>);
+
+/* twiddles of the plane geometry start at the y axis of the lattice table (offset NX) and of
+ * the pencil geometry at the x axis (offset 0): both are e^{-2 pi i t/n} per axis */
+static int big_derivs(double2 *in, int nf, double2 *lap, double2 *dx, double2 *dy, double2 *dz,
+                      const double2 *tw, const double *ktab, cudaStream_t st)
+{
+    constexpr int NYZ = NY * NZ, N = NX * NY * NZ;
+    if (NYZ % WTD_PX != 0) return WTD_ERR_UNSUPPORTED;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_planes<WGP, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)planes_smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_planes<WGP, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)planes_smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_pencils<WGX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pencils_smem) != cudaSuccess)
+            return WTD_ERR_CUDA;
+        attr = true;
+    }
+    /* forward (y, z) into the laplacian buffer (in place when there is none: the input is then
+     * overwritten by its transform) */
+    double2 *K = lap ? lap : in;
+    k_planes<WGP, -1><<<nf * NX, 512, planes_smem, st>>>(in, K, NX, tw + NX, ktab);
+    k_pencils<WGX><<<nf * (NYZ / WTD_PX), 512, pencils_smem, st>>>(K, lap, dx, dy, dz, NYZ, N, tw, ktab);
+    double2 *outs[4] = {lap, dx, dy, dz};
+    for (int k = 0; k < 4; k++)
+        if (outs[k]) k_planes<WGP, +1><<<nf * NX, 512, planes_smem, st>>>(outs[k], outs[k], NX, tw + NX, ktab);
+    return cudaGetLastError() == cudaSuccess ? WTD_OK : WTD_ERR_CUDA;
+}
+
+/* real field -> laplacian or d/dx_d of it (complex staging buffer of N points) */
+__global__ void k_real_to_c(const double *f, double2 *c, int n)
+{
+    int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i < n) c[i] = make_double2(f[i], 0.0);
+}
+__global__ void k_c_to_real(const double2 *c, double *f, int n, double scale, int accumulate)
+{
+    int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i < n) f[i] = accumulate ? f[i] + scale * c[i].x : scale * c[i].x;
+}
+/* tau = max(0, lap(rho)/2 - tau_tmp) from the staged laplacian (pca_dens.cu:275-290) */
+__global__ void k_tau_from_lap(const double2 *lap, double *tau, int n)
+{
+    int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i >= n) return;
+    double t = 0.5 * lap[i].x - tau[i];
+    tau[i] = t < 0.0 ? 0.0 : t;
+}
+
+/* out (+)= scale * op(f) for a real field: which 0 = laplacian, 1..3 = d/dx, d/dy, d/dz.
+ * stage holds 2N complex numbers of scratch. */
+static int big_real_deriv(const double *f, double *out, int which, double scale, int accumulate, double2 *stage,
+                          const double2 *tw, const double *kt, cudaStream_t st)
+{
+    constexpr int N = NX * NY * NZ;
+    const int nb = (N + 255) / 256;
+    k_real_to_c<<<nb, 256, 0, st>>>(f, stage, N);
+    double2 *res = stage;
+    int r;
+    if (which == 0) r = big_derivs(stage, 1, stage, NULL, NULL, NULL, tw, kt, st);
+    else {
+        res = stage + N;
+        r = big_derivs(stage, 1, NULL, which == 1 ? res : NULL, which == 2 ? res : NULL, which == 3 ? res : NULL, tw, kt, st);
+    }
+    if (r) return r;
+    k_c_to_real<<<nb, 256, 0, st>>>(res, out, N, scale, accumulate);
+    return cudaGetLastError() == cudaSuccess ? WTD_OK : WTD_ERR_CUDA;
+}
+
+/* tau of both spins on a large lattice */
+static int big_tau(double *dens, double2 *stage, const double2 *tw, const double *kt, cudaStream_t st)
+{
+    constexpr int N = NX * NY * NZ;
+    const int nb = (N + 255) / 256;
+    for (int s = 0; s < 2; s++) {
+        k_real_to_c<<<nb, 256, 0, st>>>(dens + (s == 0 ? 2 : 7) * (size_t)N, stage, N);
+        int r = big_derivs(stage, 1, stage, NULL, NULL, NULL, tw, kt, st);
+        if (r) return r;
+        k_tau_from_lap<<<nb, 256, 0, st>>>(stage, dens + (s == 0 ? 3 : 8) * (size_t)N, N);
+    }
+    return cudaGetLastError() == cudaSuccess ? WTD_OK : WTD_ERR_CUDA;
+}
+
+/* variable mass on a large lattice: CF_NA/NB = lap(alpha)/4, CF_CJA/CJB = -div(A)/2
+ * (pca_kernels.cu:778-795), from the CF_ALA.. / CF_AAX.. rows already in cf */
+static int big_prep_var(double *cf, double2 *stage, const double2 *tw, const double *kt, cudaStream_t st)
+{
+    constexpr size_t N = (size_t)NX * NY * NZ;
+    for (int s = 0; s < 2; s++) {
+        WTD_TRY(big_real_deriv(cf + (s == 0 ? CF_ALA : CF_ALB) * N, cf + (s == 0 ? CF_NA : CF_NB) * N, 0, 0.25, 0, stage, tw, kt, st));
+        for (int d = 0; d < 3; d++)
+            WTD_TRY(big_real_deriv(cf + ((s == 0 ? CF_AAX : CF_ABX) + d) * N, cf + (s == 0 ? CF_CJA : CF_CJB) * N, d + 1, -0.5,
+                                   d > 0, stage, tw, kt, st));
+    }
+    return WTD_OK;
+}
+
+#endif

@@ -14,6 +14,8 @@
 #include "wtd_surface.h"
 #include "problem-definition.h"
 #include "wtd_functional.cuh"
-#include "wtd_api.cuh"
+#include "wtd_lattice.cuh"
+#include "wtd_fft3d.cuh"
 #define WTD_CODEDIM CODEDIM
 #include "wtd_compat.cuh"
+#include "wtd_api.cuh"
