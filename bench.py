@@ -14,8 +14,10 @@ Arms:
              the FP32-mixed forms and the reference's own CUDA kernels on the same GPU.
   reference  the reference's step on the host cores (the CPU oracle port, all threads), on a
              bounded sample of the same workload.
-Multi-GPU (torchrun): states are sharded over ranks (weak scaling); every rank runs its shard
-and the per-rank time is max-reduced; the density sum over shards is the step's exchange.
+Multi-GPU (torchrun): the workload's states are sharded over ranks in contiguous blocks (strong
+scaling: one physical system of a fixed state count); after every density reduction NCCL sums
+the partial densities over ranks on the context stream (the step's one exchange), and the
+per-rank device time is max-reduced.
 """
 import argparse
 import json
@@ -38,6 +40,10 @@ WORKLOADS = {
 }
 
 
+# bounded CPU samples of each workload (states, steps): about 10-30 s on the host cores
+CPU_SAMPLE = {"c2": (1024, 40), "c1": (256, 4000), "c4": (1024, 60)}
+
+
 def peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
@@ -48,10 +54,12 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """nvidia-smi clock/throttle samples during the timed region: the sampler is running (its
+    first sample seen) before the region starts, and one sample after its end is kept."""
 
     def __init__(self, index=0):
         self.index, self.samples, self.proc, self.th = index, [], None, None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -59,21 +67,30 @@ class ClockSampler:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.th = threading.Thread(target=self._read, daemon=True)
             self.th.start()
+            t_wait = time.monotonic() + 5.0
+            while not self.samples and time.monotonic() < t_wait:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.t0 = time.monotonic()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) >= 7:
-                self.samples.append(parts)
+                self.samples.append((time.monotonic(), parts))
 
     def __exit__(self, *a):
+        self.t1 = time.monotonic()
         if self.proc:
+            n = len(self.samples)
+            t_wait = time.monotonic() + 1.0
+            while len(self.samples) == n and time.monotonic() < t_wait:
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -81,14 +98,16 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.samples:
+        inside = [p for t, p in self.samples if self.t0 is not None and t >= self.t0]
+        if not inside:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        sm = [float(s[0]) for s in inside if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in inside if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].strip() == "Active"})
+        reasons = sorted({names[k] for s in inside for k in range(4) if s[3 + k].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(inside),
+                "timed_region_s": round((self.t1 or self.t0) - self.t0, 3)}
 
 
 def make_inputs(name, nwf, device_qr=True):
@@ -132,16 +151,25 @@ def run_wtd(args, rank, world):
     wl = WORKLOADS[args.workload]
     name = wl["project"]
     nwf_total = args.nwf or wl["nwf"]
-    nwf = nwf_total // world  # states sharded over ranks; per-rank work fixed by the config
     torch.cuda.set_device(rank % max(1, torch.cuda.device_count()))
     dev = torch.cuda.current_device()
-    proj, d = make_inputs(name, nwf)
+    proj, d = make_inputs(name, nwf_total)
+    if world > 1:
+        # one system of nwf_total states, a contiguous block per rank (getnwfip); the density
+        # partials are summed over ranks by NCCL after every density reduction
+        from wslda_b200.sharding import shard_rows, shard_vector
+        d["states"] = shard_rows(d["states"], nwf_total, proj.numel, world, rank)
+        d["occ"] = shard_vector(d["occ"], nwf_total, world, rank)
+    nwf = len(d["occ"])
     res = {}
     forms = [("fp64", 0)] + ([("mixed_h64", 1), ("mixed_h32", 2)] if not args.fp64_only else [])
     base_precision = 0
     for label, prec in forms:
         r = TDRun(name, nwf, precision=prec, device=dev)
         r.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+        if world > 1:
+            from wslda_b200.sharding import attach_nccl
+            attach_nccl(r, rank, world)
         r.initial_measurement()
         r.steps(args.warmup)
         r.sync()
@@ -186,9 +214,44 @@ def run_wtd(args, rank, world):
             e2e_ms = e0.elapsed_time(e1)
             wall = (time.perf_counter() - t0) * 1e3
             res["e2e"] = dict(ms=max(e2e_ms, 0.0), wall_ms=wall, h2d=hst.numel() * 8, d2h=hd.numel() * 8 + 11 * 8)
+        if label == "fp64" and world == 1 and (args.adjoint or args.workload == "c4") and proj.cfg.get("stirrer_params"):
+            res["adjoint"] = time_adjoint(r, proj, d, stream, args.adjoint_steps)
         r.close()
     return proj, nwf, res
 
+
+def time_adjoint(r, proj, d, stream, steps=0):
+    """device time of the loss-only forward and of the gradient call (forward, segment
+    recompute, reverse sweep) over the project's optimal-control horizon: with the checkpoint
+    interval chosen by the library (0: records of every step when they fit) and with the
+    project's interval; each gradient timed on its second call (workspace already allocated)"""
+    import torch
+    ns = steps or proj.cfg.get("steps", 200)
+    K = min(proj.cfg.get("checkpoint_every", 20), ns)
+    npar = proj.cfg["stirrer_params"]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(**kw):
+        r.upload_states(d["states"])
+        torch.cuda.synchronize()
+        e0.record(stream)
+        loss, g = r.adjoint(ns, **kw)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), loss, g
+
+    timed()
+    tf, loss, _ = timed()
+    out = {"steps": ns, "nparam": npar, "ms_forward_with_loss": tf}
+    for label, k in (("auto", 0), (f"K{K}", K)):
+        t_first = timed(nparam=npar, checkpoint_every=k)[0]
+        tg, loss_g, g = timed(nparam=npar, checkpoint_every=k)
+        out[label] = {"checkpoint_every": k or "auto", "ms_gradient": tg, "ms_first_call": t_first,
+                      "gradient_over_forward": tg / tf}
+        r.adjoint_release()
+    out["loss"] = loss
+    out["grad_norm"] = float(np.linalg.norm(g))
+    return out
 
 def reference_cuda(name, nwf, steps):
     """The reference's own kernels (hpc-engine/*.cu built for sm_100a) on the same GPU."""
@@ -242,6 +305,8 @@ def main():
     ap.add_argument("--nwf", type=int, default=0, help="override the workload's state count (small profiling cases)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-refcuda", action="store_true")
+    ap.add_argument("--adjoint", action="store_true", help="also time the adjoint gradient (stirrer projects)")
+    ap.add_argument("--adjoint-steps", type=int, default=0, help="adjoint horizon (default: the project's steps)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -254,7 +319,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        sample = {"c2": (1024, 4), "c1": (256, 20), "c4": (1024, 6)}[args.workload]
+        sample = CPU_SAMPLE[args.workload]
         vals = []
         for _ in range(args.warmup if False else 0):
             pass
@@ -267,7 +332,7 @@ def main():
         cb["value"] = v
         line = {"impl": "reference", "metric": metric, "value": v, "unit": metric, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": wl["nwf"] / v * 1e3,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": cfg, "cpu_baseline": cb,
                 "e2e": {"value": v, "unit": metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "note": "the reference has no CPU implementation of the TD step (td codes require GPUs); this arm "
@@ -280,6 +345,7 @@ def main():
         import torch
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     proj, nwf, res = run_wtd(args, rank, world)
+    nwf_total = args.nwf or wl["nwf"]
     if rank != 0:
         if world > 1:
             import torch
@@ -287,12 +353,12 @@ def main():
         return
     hbm, peak_kind = peaks()
     f = res["fp64"]
-    value = nwf * world * args.steps / (f["ms"] * 1e-3)
+    value = nwf_total * args.steps / (f["ms"] * 1e-3)
     ba, bb = pass_bytes(proj, 0)
     achieved = ba * nwf / (f["ms_a"] * 1e-3) / 1e9
     line = {
         "metric": metric, "value": value, "unit": metric, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": f["ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": f["ms"] / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded PCG64 Gaussian states, QR-orthonormalised)", "config": cfg,
         "gpu_launches": int(f["launches"]),
         "roofline": {"bound": "hbm", "kernel": "wtd_fused_pass<PASS=0> (H psi + ABM predictor)",
@@ -305,7 +371,7 @@ def main():
     }
     if "e2e" in res:
         e = res["e2e"]
-        line["e2e"] = {"value": nwf * world * args.steps / (e["ms"] * 1e-3), "unit": metric,
+        line["e2e"] = {"value": nwf_total * args.steps / (e["ms"] * 1e-3), "unit": metric,
                        "h2d_bytes_per_step": e["h2d"] / args.steps, "d2h_bytes_per_step": e["d2h"] / args.steps,
                        "ms": e["ms"], "definition": "upload states (pinned) + initial measurement + K steps + "
                        "download densities + energy, per K steps"}
@@ -317,13 +383,15 @@ def main():
             n = proj.numel
             rho = np.concatenate([d64[2 * n:3 * n], d64[7 * n:8 * n]])
             rho_m = np.concatenate([m["dens"][2 * n:3 * n], m["dens"][7 * n:8 * n]])
-            forms[label] = {"value": nwf * world * args.steps / (m["ms"] * 1e-3),
+            forms[label] = {"value": nwf_total * args.steps / (m["ms"] * 1e-3),
                             "speedup_vs_fp64": f["ms"] / m["ms"],
                             "density_rel_l2_err_vs_fp64": float(np.linalg.norm(rho_m - rho) / np.linalg.norm(rho)),
                             "energy_rel_err_vs_fp64": float(abs(m["energy"][:7].sum() - f["energy"][:7].sum()) / abs(f["energy"][:7].sum())),
                             "ms_pass_a": m["ms_a"], "ms_pass_b": m["ms_b"]}
     if forms:
         line["precision_forms"] = forms
+    if "adjoint" in res:
+        line["adjoint"] = res["adjoint"]
     if not args.no_refcuda and world == 1:
         try:
             line["reference_cuda"] = reference_cuda(proj.name, nwf, max(2, min(args.steps, 10)))
@@ -332,7 +400,7 @@ def main():
         except Exception as ex:  # reported, not fatal
             line["reference_cuda"] = {"error": str(ex)[:200]}
     if not args.no_cpu and world == 1:
-        sample = {"c2": (1024, 4), "c1": (256, 20), "c4": (1024, 6)}[args.workload]
+        sample = CPU_SAMPLE[args.workload]
         line["cpu_baseline"] = cpu_baseline(proj.name, *sample)
     print(json.dumps(line))
     if world > 1:

@@ -54,6 +54,7 @@ typedef struct wtd_ctx wtd_ctx;
 #define WTD_ERR_UNSUPPORTED -3
 #define WTD_ERR_STATE -4
 #define WTD_ERR_NOMEM -5
+#define WTD_ERR_COMM -7   /* density exchange failed (NCCL missing or a collective error) */
 
 /* lattice and build facts of this library: dims[3], numel, codedim, scheme history length,
  * functional id (111 SLDA, 112 ASLDA, 113 BDG, 114 CUSTOMEDF), const-mass flag */
@@ -110,6 +111,41 @@ long long wtd_launch_count(wtd_ctx *ctx);
  * launch): enable, then read the summed milliseconds and launch counts since the last read */
 int wtd_set_timing(wtd_ctx *ctx, int on);
 int wtd_pass_times(wtd_ctx *ctx, double *ms_pass_a, double *ms_pass_b, int *count_a, int *count_b);
+
+/* Optimal-control gradient (no counterpart in the reference, which has no adjoint).
+ * From the states currently uploaded, runs wtd_initial_measurement(it0) and nsteps steps and
+ * returns L = sum_r |Delta(r, T)|^2 mask(r) dV of the final pairing field (mask NULL = 1).
+ * With grad non-NULL it also returns dL/dparams[j], j < nparam, through a hand-written
+ * adjoint of the step: the forward keeps a checkpoint every checkpoint_every steps (0: the
+ * largest interval whose step records fit in free device memory, all nsteps when they do),
+ * records the last segment as it runs, and the reverse sweep recomputes each earlier segment
+ * once.  Requires a contact-BdG project (Delta = -g nu, V = v_ext; WTD_ADJOINT_CONTACT_BDG
+ * names the params index of g), constant mass, FP64 and a lattice on the fused path;
+ * otherwise WTD_ERR_UNSUPPORTED.  The context is left as after the forward; its device
+ * workspace is kept for the next call until wtd_adjoint_release or wtd_destroy. */
+int wtd_adjoint(wtd_ctx *ctx, int it0, int nsteps, int checkpoint_every, const double *mask, int nparam,
+                double *loss, double *grad);
+int wtd_adjoint_release(wtd_ctx *ctx);
+
+/* ---- state-sharded runs (one process per GPU, each context holding a block of the states) ----
+ * Densities are sums over states, so every density reduction of a sharded run is followed by a
+ * sum over ranks: the reference's MPI_Allreduce of d_densities (hpc-engine/pca.c:948, 1433,
+ * 1505).  Each context then holds the full densities and computes the same potentials.
+ * Either attach an NCCL communicator (the sum runs on the context stream, no host sync), or
+ * register a host hook (e.g. MPI after a stream sync).  Without either, the context's own
+ * states are the whole system. */
+
+/* NCCL: a 128-byte ncclUniqueId made on one rank and sent to all (any channel), then
+ * wtd_nccl_attach on every rank.  libnccl.so.2 is loaded at run time (the process's copy if
+ * one is already loaded). */
+int wtd_nccl_unique_id(void *id128);
+int wtd_nccl_attach(wtd_ctx *ctx, const void *id128, int nranks, int rank);
+
+/* host hook: called after each density reduction with the device array of count doubles
+ * (partial sums of this rank's states) and the context's cudaStream_t; it must leave the sum
+ * over ranks in place, ordered on that stream, and return 0.  fn NULL removes the hook. */
+typedef int (*wtd_exchange_fn)(void *user, double *dens, size_t count, void *stream);
+int wtd_set_density_exchange(wtd_ctx *ctx, wtd_exchange_fn fn, void *user);
 
 #ifdef __cplusplus
 }

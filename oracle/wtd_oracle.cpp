@@ -56,6 +56,15 @@ static std::vector<double> dens, pots, fb, kky, kkz, qpe, work;
 static std::vector<int> cnt;
 static std::vector<unsigned char> extra;
 static int last_gradients = 0;
+/* state-sharded runs: sum of the density partials over ranks, after each density reduction
+ * (the reference's MPI_Allreduce of the densities, pca.c:948, 1433, 1505) */
+typedef int (*exchange_fn)(void *user, double *dens, size_t count);
+static exchange_fn xfn = nullptr;
+static void *xuser = nullptr;
+static void exchange_densities()
+{
+    if (xfn) xfn(xuser, dens.data(), dens.size());
+}
 
 /* point coordinates of linear index i (pca_macro.h:134-160) */
 static inline void decode(int i, int &ix, int &iy, int &iz)
@@ -669,6 +678,7 @@ static void half_step_densities(int it_next, int grads)
 {
     derivatives(y, grads);
     calculate_densities(y, grads);
+    exchange_densities();
     if (grads) density_tau();
     compute_potentials(it_next);
     alpha_laplace(y);
@@ -752,6 +762,7 @@ int orc_initial_measurement(void)
     normalize(y);
     derivatives(y, 1);
     calculate_densities(y, 1);
+    exchange_densities();
     density_tau();
     last_gradients = 1;
     return 0;
@@ -864,6 +875,12 @@ int orc_get_history(int slot, double *out)
     return 0;
 }
 int orc_get_it(void) { return it_global; }
+int orc_set_density_exchange(exchange_fn fn, void *user)
+{
+    xfn = fn;
+    xuser = user;
+    return 0;
+}
 int orc_set_threads(int n)
 {
 #ifdef _OPENMP

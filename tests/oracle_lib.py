@@ -22,6 +22,14 @@ def build(project):
     return so
 
 
+def _stale(so):
+    if not os.path.exists(so):
+        return True
+    t = os.path.getmtime(so)
+    srcs = [os.path.join(ORACLE_DIR, f) for f in ("wtd_oracle.cpp", "oracle_surface.h", "oracle_edf.h")]
+    return any(os.path.exists(f) and os.path.getmtime(f) > t for f in srcs)
+
+
 class Oracle:
     """One oracle instance per project (a separate process-level library, as it keeps state)."""
 
@@ -29,7 +37,7 @@ class Oracle:
         from wslda_b200.projects import Project
         self.proj = Project(project)
         so = os.path.join(ORACLE_DIR, "_build", project, "liboracle.so")
-        if not os.path.exists(so):
+        if _stale(so):
             build(project)
         self.lib = ctypes.CDLL(so, mode=ctypes.RTLD_LOCAL)
         L = self.lib
@@ -48,6 +56,8 @@ class Oracle:
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_fft_field.argtypes = [_dp, ctypes.c_int]
         L.orc_derivatives_field.argtypes = [_dp] * 5
+        L.orc_set_density_exchange.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._xfn = None
         if threads:
             L.orc_set_threads(int(threads))
         self.N = L.orc_numel()
@@ -70,6 +80,22 @@ class Oracle:
 
     def initial_measurement(self):
         return self.lib.orc_initial_measurement()
+
+    def set_density_exchange(self, fn):
+        """fn(dens) with dens a numpy view of the 12N partial densities, summed in place over
+        ranks (None removes the hook)"""
+        if fn is None:
+            self._xfn = None
+            self.lib.orc_set_density_exchange(None, None)
+            return
+        proto = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t)
+
+        def tramp(_user, ptr, count):
+            fn(np.ctypeslib.as_array(ptr, shape=(count,)))
+            return 0
+
+        self._xfn = proto(tramp)
+        self.lib.orc_set_density_exchange(ctypes.cast(self._xfn, ctypes.c_void_p), None)
 
     def steps(self, n):
         return self.lib.orc_steps(int(n))

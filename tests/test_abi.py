@@ -14,6 +14,7 @@ def declared_symbols():
     for h in HEADERS:
         src = open(h).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        src = re.sub(r"^\s*typedef[^;]*;", "", src, flags=re.M)  # function-pointer types are not exports
         for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_\s\*]*?\b([a-z_][a-z0-9_]*)\s*\(", src, flags=re.M):
             if m.group(1) not in ("if", "sizeof", "defined"):
                 names.add(m.group(1))

@@ -51,7 +51,15 @@ SIGNATURES = {
     "wtd_launch_count": (ctypes.c_longlong, [ctypes.c_void_p]),
     "wtd_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "wtd_pass_times": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _ip, _ip]),
+    "wtd_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp]),
+    "wtd_adjoint_release": (ctypes.c_int, [ctypes.c_void_p]),
+    "wtd_nccl_unique_id": (ctypes.c_int, [ctypes.c_void_p]),
+    "wtd_nccl_attach": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "wtd_set_density_exchange": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
 }
+
+# host hook of a state-sharded run: int fn(void *user, double *dens, size_t count, void *stream)
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
 
 
 def load_library(project, build=True):
@@ -184,3 +192,55 @@ class TDRun:
         na, nb = ctypes.c_int(), ctypes.c_int()
         self._check(self.lib.wtd_pass_times(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(na), ctypes.byref(nb)))
         return a.value, b.value, na.value, nb.value
+
+    def nccl_unique_id(self):
+        """128-byte NCCL unique id (made on one rank, sent to all)"""
+        buf = ctypes.create_string_buffer(128)
+        self._check(self.lib.wtd_nccl_unique_id(buf))
+        return buf.raw
+
+    def attach_nccl(self, uid, nranks, rank):
+        """sum the density partials over nranks contexts with NCCL on this context's stream"""
+        buf = ctypes.create_string_buffer(bytes(uid), 128)
+        self._check(self.lib.wtd_nccl_attach(self.h, buf, int(nranks), int(rank)))
+
+    def set_density_exchange(self, fn):
+        """host hook fn(dens_ptr, count, stream_ptr) -> None, called after every density
+        reduction; it must leave the sum over ranks in place (None removes the hook)"""
+        if fn is None:
+            self._xfn = None
+            self._check(self.lib.wtd_set_density_exchange(self.h, None, None))
+            return
+
+        def tramp(_user, ptr, count, stream):
+            try:
+                fn(ptr, count, stream)
+                return 0
+            except Exception:  # reported to the library as a failed exchange
+                import traceback
+                traceback.print_exc()
+                return 1
+
+        self._xfn = EXCHANGE_FN(tramp)
+        self._check(self.lib.wtd_set_density_exchange(self.h, ctypes.cast(self._xfn, ctypes.c_void_p), None))
+
+    def adjoint_release(self):
+        """free the adjoint's device workspace (kept between gradient calls)"""
+        self._check(self.lib.wtd_adjoint_release(self.h))
+
+    def set_params(self, params):
+        self._params = np.ascontiguousarray(params, dtype=np.float64)
+        self._check(self.lib.wtd_set_params(self.h, _p(self._params)))
+
+    def adjoint(self, nsteps, nparam=0, mask=None, checkpoint_every=0, it0=None):
+        """Loss L = sum_r |Delta(r,T)|^2 mask dV after initial_measurement(it0) + nsteps steps
+        from the uploaded states, and (nparam > 0) dL/dparams[:nparam] by the adjoint sweep
+        (checkpoint_every 0: the largest interval that fits in device memory).
+        Returns (L, grad or None); the run is left at the end of the forward."""
+        loss = np.zeros(1)
+        grad = np.zeros(max(nparam, 1))
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
+        self._check(self.lib.wtd_adjoint(self.h, int(self.it0 if it0 is None else it0), int(nsteps),
+                                         int(checkpoint_every), _p(m), int(nparam), _p(loss),
+                                         _p(grad) if nparam > 0 else None))
+        return float(loss[0]), (grad[:nparam].copy() if nparam > 0 else None)

@@ -12,6 +12,8 @@
 #ifndef WTD_API_CUH
 #define WTD_API_CUH
 
+#include <dlfcn.h>
+#include <nccl.h>
 #include "wtd_lattice.cuh"
 
 struct wtd_ctx {
@@ -42,9 +44,60 @@ struct wtd_ctx {
     /* large 3D lattices (state larger than one CTA's shared memory): staged path */
     int staged;
     double2 *ddx, *ddy, *ddz, *dlap, *dalap, *stage3d;
+    /* state-sharded runs: sum of the density partials over ranks (NCCL or a host hook) */
+    void *nccl;
+    wtd_exchange_fn xfn;
+    void *xuser;
+    /* adjoint workspace kept between gradient calls (AdjWork, released with the context) */
+    void *adj;
 };
 
+static void adj_release(wtd_ctx *c);
+
 #define WTD_LAUNCHED(ctx) do { (ctx)->launches++; cudaError_t _e = cudaGetLastError(); if (_e != cudaSuccess) return WTD_ERR_CUDA; } while (0)
+
+/* ---------------------------------------------------------------------------------------
+ * density exchange of state-sharded runs.  NCCL is loaded at run time so that the library has
+ * no link-time dependency and shares the process's NCCL when one is already loaded.
+ * -------------------------------------------------------------------------------------*/
+struct NcclApi {
+    ncclResult_t (*get_unique_id)(ncclUniqueId *);
+    ncclResult_t (*comm_init_rank)(ncclComm_t *, int, ncclUniqueId, int);
+    ncclResult_t (*all_reduce)(const void *, void *, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t, cudaStream_t);
+    ncclResult_t (*comm_destroy)(ncclComm_t);
+};
+
+static const NcclApi *nccl_api()
+{
+    static NcclApi api;
+    static int state = 0; /* 0 untried, 1 loaded, -1 unavailable */
+    if (state == 0) {
+        state = -1;
+        void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+        if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
+        if (h) {
+            api.get_unique_id = (decltype(api.get_unique_id))dlsym(h, "ncclGetUniqueId");
+            api.comm_init_rank = (decltype(api.comm_init_rank))dlsym(h, "ncclCommInitRank");
+            api.all_reduce = (decltype(api.all_reduce))dlsym(h, "ncclAllReduce");
+            api.comm_destroy = (decltype(api.comm_destroy))dlsym(h, "ncclCommDestroy");
+            if (api.get_unique_id && api.comm_init_rank && api.all_reduce && api.comm_destroy) state = 1;
+        }
+    }
+    return state == 1 ? &api : NULL;
+}
+
+/* in-place sum over ranks of count doubles on the context stream (no-op for a lone context) */
+static int exchange(wtd_ctx *c, double *buf, size_t count)
+{
+    if (c->nccl) {
+        const NcclApi *a = nccl_api();
+        if (!a || a->all_reduce(buf, buf, count, ncclFloat64, ncclSum, (ncclComm_t)c->nccl, c->st) != ncclSuccess)
+            return WTD_ERR_COMM;
+    } else if (c->xfn) {
+        if (c->xfn(c->xuser, buf, count, (void *)c->st) != 0) return WTD_ERR_COMM;
+    }
+    return WTD_OK;
+}
 
 static size_t elem_bytes_y(int prec) { return prec == WTD_FP64 ? sizeof(double2) : sizeof(float2); }
 static size_t elem_bytes_h(int prec) { return prec == WTD_MIXED_H32 ? sizeof(float2) : sizeof(double2); }
@@ -146,6 +199,7 @@ static int after_pass(wtd_ctx *c, bool full, int it)
     int nb = (12 * N + 255) / 256;
     wtd_dens_reduce<<<nb, 256, 0, c->st>>>(c->dslot, c->grid, c->dens, N, full ? 1 : 0, 1.0 / WTD_LPERP);
     WTD_LAUNCHED(c);
+    WTD_TRY(exchange(c, c->dens, 12 * (size_t)N));
     if (full) {
         constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
         if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
@@ -196,6 +250,7 @@ static int staged_densities(wtd_ctx *c, bool grads)
     WTD_LAUNCHED(c);
     wtd_dens_reduce<<<(12 * N + 255) / 256, 256, 0, c->st>>>(c->dslot, G, c->dens, N, grads ? 1 : 0, 1.0 / WTD_LPERP);
     WTD_LAUNCHED(c);
+    WTD_TRY(exchange(c, c->dens, 12 * (size_t)N));
     if (grads) WTD_TRY(big_tau(c->dens, c->stage3d, c->tw, c->ktab, c->st));
     return WTD_OK;
 }
@@ -288,6 +343,60 @@ static int staged_step(wtd_ctx *c, bool last)
     return WTD_OK;
 }
 
+/* what the adjoint's reverse sweep needs of one fused step */
+struct StepRecord {
+    double2 *yk, *yp;           /* state before the step, normalised predictor state */
+    double *cfA, *cfB;          /* H coefficients of pass A and pass B */
+    double *EA, *EB, *nA, *nB;  /* <H> and update norms of both half steps */
+    int hasH;                   /* pass A formed f_k with H (0 on the first step) */
+};
+
+/* one fused step: pass A, functional, pass B, functional.
+ * rec != NULL records the step without copying states: pass A reads y_k from rec->yk and
+ * writes y_pred into rec->yp, pass B writes y_{k+1} into yk_next (the next record's yk) or,
+ * when yk_next is NULL, into the context's states. */
+static int fused_step(wtd_ctx *c, bool last, StepRecord *rec, double2 *yk_next = NULL)
+{
+    const bool var = WTD_VAR;
+    constexpr int N = WTD_NUMEL;
+    if (!c->fk_given && !c->have_coef) return WTD_ERR_STATE;
+    if (rec) {
+        WTD_CU(cudaMemcpyAsync(rec->cfA, c->cf, CF_COUNT * (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+        rec->hasH = c->fk_given ? 0 : 1;
+    }
+    /* predictor: f_k, y_pred, P; densities of y_pred */
+    if (!rec) {
+        WTD_TRY(run_pass(c, 0, var));
+    } else {
+        StepArgs a = make_args(c);
+        a.y = rec->yk;
+        a.yout = rec->yp;
+        a.nrm_out = rec->nA;
+        a.qpe = rec->EA;
+        WTD_TRY((var ? launch_pass<0, true>(c, a) : launch_pass<0, false>(c, a)));
+    }
+    WTD_TRY(after_pass(c, var, c->it + 1));
+    if (rec) WTD_CU(cudaMemcpyAsync(rec->cfB, c->cf, CF_COUNT * (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    /* corrector */
+    const bool g = var || last;
+    if (!rec) {
+        WTD_TRY(run_pass(c, 1, g));
+    } else {
+        StepArgs a = make_args(c);
+        a.y = rec->yp;
+        a.yout = yk_next ? (void *)yk_next : c->y;
+        a.nrm_out = rec->nB;
+        a.qpe = rec->EB;
+        WTD_TRY((g ? launch_pass<1, true>(c, a) : launch_pass<1, false>(c, a)));
+    }
+    WTD_TRY(after_pass(c, g, c->it + 1));
+    /* ring: f_k becomes the newest history entry, P's slot becomes free */
+    c->head = (c->head + WTD_NHIST - 1) % WTD_NHIST;
+    c->fk_given = 0;
+    c->it++;
+    return WTD_OK;
+}
+
 template <typename TY, typename TH, typename TC>
 static int occupancy_t(int block)
 {
@@ -350,6 +459,7 @@ const char *wtd_error_string(int code)
     case WTD_ERR_UNSUPPORTED: return "lattice/mode not supported by this build";
     case WTD_ERR_STATE: return "call out of order";
     case WTD_ERR_NOMEM: return "out of device memory";
+    case WTD_ERR_COMM: return "density exchange failed (NCCL not loadable, or a collective or hook error)";
     case -6: return "lattice too large for the fixed scratch of calculate_densities_noalloc (12*N doubles > 1 Mi words)";
     default: return "unknown error";
     }
@@ -448,6 +558,8 @@ int wtd_destroy(wtd_ctx *c)
     if (!c) return WTD_OK;
     cudaSetDevice(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
+    adj_release(c);
+    if (c->nccl && nccl_api()) nccl_api()->comm_destroy((ncclComm_t)c->nccl);
     if (c->timing)
         for (int p = 0; p < 2; p++)
             for (int k = 0; k < 2; k++)
@@ -650,21 +762,8 @@ int wtd_steps(wtd_ctx *c, int nsteps)
         for (int s = 0; s < nsteps; s++) WTD_TRY(staged_step(c, s == nsteps - 1));
         return WTD_OK;
     }
-    for (int s = 0; s < nsteps; s++) {
-        const bool last = (s == nsteps - 1);
-        if (!c->fk_given && !c->have_coef) return WTD_ERR_STATE;
-        /* predictor: f_k, y_pred, P; densities of y_pred */
-        WTD_TRY(run_pass(c, 0, var));
-        WTD_TRY(after_pass(c, var, c->it + 1));
-        /* corrector */
-        const bool g = var || last;
-        WTD_TRY(run_pass(c, 1, g));
-        WTD_TRY(after_pass(c, g, c->it + 1));
-        /* ring: f_k becomes the newest history entry, P's slot becomes free */
-        c->head = (c->head + WTD_NHIST - 1) % WTD_NHIST;
-        c->fk_given = 0;
-        c->it++;
-    }
+    (void)var;
+    for (int s = 0; s < nsteps; s++) WTD_TRY(fused_step(c, s == nsteps - 1, NULL));
     return WTD_OK;
 }
 
@@ -769,6 +868,360 @@ int wtd_pass_times(wtd_ctx *c, double *ms_a, double *ms_b, int *count_a, int *co
 }
 long long wtd_launch_count(wtd_ctx *c) { return c ? c->launches : 0; }
 
+int wtd_nccl_unique_id(void *id128)
+{
+    if (!id128) return WTD_ERR_ARG;
+    const NcclApi *a = nccl_api();
+    ncclUniqueId id;
+    if (!a || a->get_unique_id(&id) != ncclSuccess) return WTD_ERR_COMM;
+    memcpy(id128, &id, sizeof(id));
+    return WTD_OK;
+}
+
+int wtd_nccl_attach(wtd_ctx *c, const void *id128, int nranks, int rank)
+{
+    if (!c || !id128 || nranks < 1 || rank < 0 || rank >= nranks) return WTD_ERR_ARG;
+    const NcclApi *a = nccl_api();
+    if (!a) return WTD_ERR_COMM;
+    WTD_CU(cudaSetDevice(c->dev));
+    if (c->nccl) { a->comm_destroy((ncclComm_t)c->nccl); c->nccl = NULL; }
+    ncclUniqueId id;
+    memcpy(&id, id128, sizeof(id));
+    ncclComm_t comm = NULL;
+    if (a->comm_init_rank(&comm, nranks, id, rank) != ncclSuccess) return WTD_ERR_COMM;
+    c->nccl = comm;
+    return WTD_OK;
+}
+
+int wtd_set_density_exchange(wtd_ctx *c, wtd_exchange_fn fn, void *user)
+{
+    if (!c) return WTD_ERR_ARG;
+    c->xfn = fn;
+    c->xuser = user;
+    return WTD_OK;
+}
+
 } /* extern "C" */
+
+/* ---------------------------------------------------------------------------------------
+ * adjoint (gradient of a loss of the final pairing field with respect to the parameters of
+ * the external potential): forward with checkpoints, the last segment recorded as it runs;
+ * reverse sweep over segments, recomputing each earlier segment once with records
+ * -------------------------------------------------------------------------------------*/
+#include "wtd_adjoint.cuh"
+
+#if defined(WTD_ADJOINT_CONTACT_BDG) && defined(FAST_CONST_EFFECTIVE_MASS_MODE)
+/* device allocations of the adjoint workspace, released together */
+struct AdjPool {
+    cudaStream_t st;
+    size_t bytes = 0;
+    std::vector<void *> p;
+    explicit AdjPool(cudaStream_t s) : st(s) {}
+    template <typename T> int get(T **out, size_t count)
+    {
+        void *q = NULL;
+        if (cudaMalloc(&q, count * sizeof(T) + 16) != cudaSuccess) { cudaGetLastError(); return WTD_ERR_NOMEM; }
+        p.push_back(q);
+        bytes += count * sizeof(T) + 16;
+        *out = (T *)q;
+        return WTD_OK;
+    }
+    ~AdjPool()
+    {
+        cudaStreamSynchronize(st); /* nothing queued may still use the buffers */
+        for (void *q : p) cudaFree(q);
+    }
+};
+
+/* everything a step reads of the context: states, physical history slots, coefficients,
+ * densities, potentials, <H> and the ring/time bookkeeping */
+struct Checkpoint {
+    void *y;
+    void *hist[WTD_NHIST];
+    double *cf, *dens, *pots, *qpe;
+    int head, it, fk_given, have_coef;
+};
+
+static int ck_alloc(wtd_ctx *c, AdjPool &pool, Checkpoint &k)
+{
+    constexpr size_t N = WTD_NUMEL;
+    WTD_TRY(pool.get((char **)&k.y, c->ysz));
+    for (int h = 0; h < WTD_NHIST; h++) WTD_TRY(pool.get((char **)&k.hist[h], c->hsz));
+    WTD_TRY(pool.get(&k.cf, CF_COUNT * N));
+    WTD_TRY(pool.get(&k.dens, 12 * N));
+    WTD_TRY(pool.get(&k.pots, 12 * N));
+    WTD_TRY(pool.get(&k.qpe, (size_t)c->S));
+    return WTD_OK;
+}
+
+static int ck_copy(wtd_ctx *c, bool save, Checkpoint &k)
+{
+    constexpr size_t N = WTD_NUMEL;
+    auto cp = [&](void *ctxp, void *ckp, size_t bytes) {
+        return cudaMemcpyAsync(save ? ckp : ctxp, save ? ctxp : ckp, bytes, cudaMemcpyDeviceToDevice, c->st);
+    };
+    WTD_CU(cp(c->y, k.y, c->ysz));
+    for (int h = 0; h < WTD_NHIST; h++) WTD_CU(cp(c->hist[h], k.hist[h], c->hsz));
+    WTD_CU(cp(c->cf, k.cf, CF_COUNT * N * sizeof(double)));
+    WTD_CU(cp(c->dens, k.dens, 12 * N * sizeof(double)));
+    WTD_CU(cp(c->pots, k.pots, 12 * N * sizeof(double)));
+    WTD_CU(cp(c->qpe, k.qpe, (size_t)c->S * sizeof(double)));
+    if (save) { k.head = c->head; k.it = c->it; k.fk_given = c->fk_given; k.have_coef = c->have_coef; }
+    else { c->head = k.head; c->it = k.it; c->fk_given = k.fk_given; c->have_coef = k.have_coef; }
+    return WTD_OK;
+}
+
+/* the workspace: capK step records and capCk checkpoints (capK = 0: loss only) */
+struct AdjWork {
+    AdjPool pool;
+    int capK = 0, capCk = 0;
+    std::vector<Checkpoint> ck;
+    Checkpoint fin;                 /* the forward's final state when segments are recomputed */
+    std::vector<StepRecord> rec;
+    double2 *ybar = NULL, *ypbar = NULL, *pbar = NULL, *fring[WTD_NHIST] = {};
+    double *fields = NULL, *dgrad = NULL, *tpart = NULL, *dloss = NULL, *dmask = NULL;
+    explicit AdjWork(cudaStream_t s) : pool(s) {}
+};
+
+static size_t adj_record_bytes(const wtd_ctx *c)
+{
+    return 2 * c->ysz + 2 * CF_COUNT * (size_t)WTD_NUMEL * sizeof(double) + 4 * (size_t)c->S * sizeof(double) + 96;
+}
+static size_t adj_ck_bytes(const wtd_ctx *c)
+{
+    return c->ysz + WTD_NHIST * c->hsz + (CF_COUNT + 24) * (size_t)WTD_NUMEL * sizeof(double) + (size_t)c->S * 8 + 112;
+}
+/* device bytes of a gradient workspace with K records and nck checkpoints */
+static size_t adj_bytes(const wtd_ctx *c, int K, int nck)
+{
+    size_t b = (size_t)K * adj_record_bytes(c) + (size_t)(nck > 0 ? nck + 1 : 0) * adj_ck_bytes(c);
+    if (K > 0) b += (3 + WTD_NHIST) * c->ysz;
+    return b + 8 * (size_t)WTD_NUMEL * sizeof(double) + (1 << 16);
+}
+
+static void adj_release(wtd_ctx *c)
+{
+    delete (AdjWork *)c->adj;
+    c->adj = NULL;
+}
+
+/* a workspace for K records and nck checkpoints: the cached one if large enough */
+static int adj_workspace(wtd_ctx *c, int K, int nck, AdjWork **out)
+{
+    AdjWork *w = (AdjWork *)c->adj;
+    if (w && w->capK >= K && w->capCk >= nck) { *out = w; return WTD_OK; }
+    const int capK = w ? (K > w->capK ? K : w->capK) : K, capCk = w ? (nck > w->capCk ? nck : w->capCk) : nck;
+    adj_release(c);
+    w = new AdjWork(c->st);
+    c->adj = w;
+    constexpr size_t N = WTD_NUMEL;
+    const size_t NS = (size_t)2 * c->S * N;
+    int r = WTD_OK;
+    auto get = [&](auto **p, size_t n) { if (r == WTD_OK) r = w->pool.get(p, n); };
+    get(&w->dloss, 1);
+    get(&w->fields, 4 * N);
+    get(&w->dmask, N);
+    get(&w->dgrad, (size_t)MAX_USER_PARAMS);
+    get(&w->tpart, (size_t)MAX_USER_PARAMS * WTD_THETA_CHUNKS);
+    if (capK > 0) {
+        get(&w->ybar, NS);
+        get(&w->ypbar, NS);
+        get(&w->pbar, NS);
+        for (int j = 0; j < WTD_NHIST; j++) get(&w->fring[j], NS);
+        w->rec.resize(capK);
+        for (auto &q : w->rec) {
+            get(&q.yk, NS);
+            get(&q.yp, NS);
+            get(&q.cfA, CF_COUNT * N);
+            get(&q.cfB, CF_COUNT * N);
+            double *sc = NULL;
+            get(&sc, 4 * (size_t)c->S);
+            q.EA = sc; q.EB = sc ? sc + c->S : NULL; q.nA = sc ? sc + 2 * c->S : NULL; q.nB = sc ? sc + 3 * c->S : NULL;
+        }
+    }
+    if (capCk > 0) {
+        w->ck.resize(capCk);
+        for (auto &k : w->ck) if (r == WTD_OK) r = ck_alloc(c, w->pool, k);
+        if (r == WTD_OK) r = ck_alloc(c, w->pool, w->fin);
+    }
+    if (r != WTD_OK) { adj_release(c); return r; }
+    w->capK = capK;
+    w->capCk = capCk;
+    *out = w;
+    return WTD_OK;
+}
+
+/* checkpoint interval: the caller's, or (0) the largest that fits in free device memory —
+ * nsteps itself (one segment, no recompute) when the records of every step fit */
+static int adj_choose_K(wtd_ctx *c, int nsteps, int K)
+{
+    if (K > 0) return K < nsteps ? K : nsteps;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return -1;
+    if (c->adj) fr += ((AdjWork *)c->adj)->pool.bytes;
+    const size_t margin = ((size_t)1 << 30) + tot / 50;
+    const size_t budget = fr > margin ? fr - margin : 0;
+    for (int k = nsteps; k >= 1; k--) {
+        const int nck = (nsteps + k - 1) / k - 1;
+        if (adj_bytes(c, k, nck) <= budget) return k;
+    }
+    return -1;
+}
+
+static int adjoint_run(wtd_ctx *c, int it0, int nsteps, int Kin, const double *mask_h, int nparam, double *loss_h,
+                       double *grad_h)
+{
+    constexpr int N = WTD_NUMEL, NH = WTD_NHIST;
+    const int S = c->S;
+    const size_t NS = (size_t)2 * S * N;
+    constexpr size_t sm = 2 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>) +
+                          80 * sizeof(double);
+    if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+    const bool grad = grad_h != NULL;
+    const int K = grad ? adj_choose_K(c, nsteps, Kin) : 0;
+    if (grad && K < 1) return WTD_ERR_NOMEM;
+    const int nseg = grad ? (nsteps + K - 1) / K : 1;
+    const int last0 = (nseg - 1) * K; /* first step of the last segment, recorded by the forward */
+    AdjWork *w = NULL;
+    WTD_TRY(adj_workspace(c, K, grad ? nseg - 1 : 0, &w));
+    double *vbar = w->fields;
+    double2 *nubar = (double2 *)(w->fields + 2 * (size_t)N);
+    if (mask_h) WTD_CU(cudaMemcpyAsync(w->dmask, mask_h, N * sizeof(double), cudaMemcpyHostToDevice, c->st));
+
+    /* forward from the uploaded states */
+    std::vector<int> itk(K > 0 ? K : 1);
+    WTD_TRY(wtd_initial_measurement(c, it0));
+    for (int s = 0; s < nsteps; s++) {
+        StepRecord *r = NULL;
+        if (grad && s < last0 && s % K == 0) WTD_TRY(ck_copy(c, true, w->ck[s / K]));
+        double2 *next = NULL;
+        if (grad && s >= last0) {
+            const int j = s - last0;
+            r = &w->rec[j];
+            itk[j] = c->it;
+            if (j == 0) WTD_CU(cudaMemcpyAsync(r->yk, c->y, c->ysz, cudaMemcpyDeviceToDevice, c->st));
+            if (s + 1 < nsteps) next = w->rec[j + 1].yk;
+        }
+        WTD_TRY(fused_step(c, s == nsteps - 1, r, next));
+    }
+    k_adj_loss<<<1, 512, 0, c->st>>>(c->pots, mask_h ? w->dmask : NULL, nubar, w->dloss);
+    WTD_LAUNCHED(c);
+    WTD_CU(cudaMemcpyAsync(loss_h, w->dloss, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    if (!grad) return wtd_cuerr(cudaStreamSynchronize(c->st));
+
+    /* reverse sweep */
+    if (nseg > 1) WTD_TRY(ck_copy(c, true, w->fin));
+    for (int j = 0; j < NH; j++) WTD_CU(cudaMemsetAsync(w->fring[j], 0, NS * sizeof(double2), c->st));
+    WTD_CU(cudaMemsetAsync(w->ybar, 0, NS * sizeof(double2), c->st));
+    WTD_CU(cudaMemsetAsync(w->dgrad, 0, MAX_USER_PARAMS * sizeof(double), c->st));
+    auto theta_grad = [&](int it) -> int {
+        if (nparam <= 0) return WTD_OK;
+        k_theta_grad<<<dim3(nparam, WTD_THETA_CHUNKS), 256, 0, c->st>>>(vbar, it, w->tpart);
+        WTD_LAUNCHED(c);
+        k_theta_sum<<<1, ((nparam + 31) / 32) * 32, 0, c->st>>>(w->tpart, nparam, WTD_THETA_CHUNKS, w->dgrad);
+        WTD_LAUNCHED(c);
+        return WTD_OK;
+    };
+    auto kB = k_adj_B<WG, NH>;
+    auto kA = k_adj_A<WG, NH>;
+    static bool attr = false;
+    if (!attr) {
+        WTD_CU(cudaFuncSetAttribute(kB, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        WTD_CU(cudaFuncSetAttribute(kA, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        attr = true;
+    }
+    /* the reverse kernels: one persistent CTA of 512 threads per SM (two CTAs of 256 per SM
+     * measured the same); the slots hold c->grid * 12 N words, so up to 3 * c->grid CTAs of 4 N */
+    const int threads = WG::ntot >= 512 ? 512 : ((WG::ntot + 31) / 32) * 32;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev);
+    int agrid = nsm;
+    if (agrid > 3 * c->grid) agrid = 3 * c->grid;
+    if (agrid > S) agrid = S;
+    const int nb = (N + 255) / 256;
+    AdjArgs base;
+    memset(&base, 0, sizeof(base));
+    base.occ = c->occ; base.kp2 = c->kp2; base.wcnt = c->wcnt;
+    base.slots = c->dslot; base.dt = c->dt; base.inv_lperp = 1.0 / WTD_LPERP; base.S = S;
+    base.ybar = w->ybar; base.ypbar = w->ypbar; base.pbar = w->pbar;
+    double2 *fring[NH];
+    for (int q = 0; q < NH; q++) fring[q] = w->fring[q];
+    bool pending = true; /* nubar holds the loss seed, the adjoint of nu(y_T) */
+    for (int sg = nseg - 1; sg >= 0; sg--) {
+        const int len = (sg == nseg - 1) ? nsteps - sg * K : K;
+        if (sg < nseg - 1) {
+            /* recompute this segment from its checkpoint, recording every step */
+            WTD_TRY(ck_copy(c, false, w->ck[sg]));
+            WTD_CU(cudaMemcpyAsync(w->rec[0].yk, c->y, c->ysz, cudaMemcpyDeviceToDevice, c->st));
+            for (int j = 0; j < len; j++) {
+                itk[j] = c->it;
+                WTD_TRY(fused_step(c, false, &w->rec[j], j + 1 < len ? w->rec[j + 1].yk : NULL));
+            }
+        }
+        for (int j = len - 1; j >= 0; j--) {
+            const StepRecord &r = w->rec[j];
+            AdjArgs b = base;
+            b.y1 = (j == len - 1) ? (const double2 *)c->y : w->rec[j + 1].yk;
+            b.yp = r.yp; b.nubar = pending ? nubar : NULL;
+            b.nrm = r.nB; b.E = r.EB; b.cf = r.cfB;
+            kB<<<agrid, threads, sm, c->st>>>(b, c->tw, c->ktab);
+            WTD_LAUNCHED(c);
+            k_adj_reduce<<<nb, 256, 0, c->st>>>(c->dslot, agrid, vbar, nubar);
+            WTD_LAUNCHED(c);
+            WTD_TRY(exchange(c, w->fields, 4 * (size_t)N));
+            WTD_TRY(theta_grad(itk[j] + 1));
+            AdjArgs a = base;
+            a.y1 = r.yk; a.yp = r.yp; a.nubar = nubar;
+            a.nrm = r.nA; a.E = r.EA; a.cf = r.cfA; a.has_h = r.hasH;
+            for (int q = 0; q < NH; q++) a.fring[q] = fring[q];
+            kA<<<agrid, threads, sm, c->st>>>(a, c->tw, c->ktab);
+            WTD_LAUNCHED(c);
+            if (r.hasH) {
+                k_adj_reduce<<<nb, 256, 0, c->st>>>(c->dslot, agrid, vbar, nubar);
+                WTD_LAUNCHED(c);
+                WTD_TRY(exchange(c, w->fields, 4 * (size_t)N));
+                WTD_TRY(theta_grad(itk[j]));
+            }
+            pending = r.hasH != 0;
+            /* the ring moves one step back: fbar_{k-1} becomes position 0 */
+            double2 *f0 = fring[0];
+            for (int q = 0; q < NH - 1; q++) fring[q] = fring[q + 1];
+            fring[NH - 1] = f0;
+            WTD_CU(cudaMemsetAsync(f0, 0, NS * sizeof(double2), c->st));
+        }
+    }
+    if (nseg > 1) WTD_TRY(ck_copy(c, false, w->fin));
+    WTD_CU(cudaMemcpyAsync(grad_h, w->dgrad, nparam * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    return wtd_cuerr(cudaStreamSynchronize(c->st));
+}
+#else
+static void adj_release(wtd_ctx *c) { (void)c; }
+#endif
+
+extern "C" int wtd_adjoint(wtd_ctx *c, int it0, int nsteps, int checkpoint_every, const double *mask, int nparam,
+                           double *loss, double *grad)
+{
+    if (!c || !loss || nsteps < 1 || checkpoint_every < 0 || nparam < 0 || nparam > MAX_USER_PARAMS ||
+        (grad && nparam < 1))
+        return WTD_ERR_ARG;
+#if defined(WTD_ADJOINT_CONTACT_BDG) && defined(FAST_CONST_EFFECTIVE_MASS_MODE)
+    if (c->prec != WTD_FP64 || c->staged) return WTD_ERR_UNSUPPORTED;
+    WTD_CU(cudaSetDevice(c->dev));
+    const int r = adjoint_run(c, it0, nsteps, checkpoint_every, mask, nparam, loss, grad);
+    if (r != WTD_OK) cudaStreamSynchronize(c->st);
+    return r;
+#else
+    (void)it0; (void)mask; (void)grad;
+    return WTD_ERR_UNSUPPORTED;
+#endif
+}
+
+extern "C" int wtd_adjoint_release(wtd_ctx *c)
+{
+    if (!c) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    adj_release(c);
+    return WTD_OK;
+}
 
 #endif

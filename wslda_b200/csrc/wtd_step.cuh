@@ -55,6 +55,7 @@ enum {
 
 struct StepArgs {
     void *y;            /* [2S][N] TY */
+    void *yout;         /* where the pass writes the updated states (NULL: in place into y) */
     void *slot[5];      /* history ring, [2S][N] TH each, indexed by ring position */
     const double *cf;   /* [CF_COUNT][N] */
     const double *occ;  /* f_n */
@@ -62,6 +63,7 @@ struct StepArgs {
     const double *wcnt; /* per-state degeneracy weight */
     double *dslot;      /* [grid][12][N] density partial sums */
     double *qpe;        /* [S] <H> of the last H application */
+    double *nrm_out;    /* [S] norm of the unnormalised update (nullable; the adjoint records it) */
     double dt;
     int S;
     int fk_given;       /* pass A: f_k is already in ring slot NH-1 */
@@ -391,6 +393,7 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
     load_tables<G>(tw, kt, gtw, gk);
 
     TY *Y = (TY *)a.y;
+    TY *YO = a.yout ? (TY *)a.yout : Y;
     const uint64_t pol = l2_policy_keep();
     double *ds = a.dslot + (size_t)blockIdx.x * 12 * N;
     if (!a.accumulate)
@@ -401,6 +404,7 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
     constexpr int NR = (PASS == 0) ? NH - 1 : (PASS == 1 ? 1 : 0); /* history arrays read per element */
     for (int n = blockIdx.x; n < a.S; n += gridDim.x) {
         TY *yu = Y + (size_t)n * N, *yv = Y + SN + (size_t)n * N;
+        TY *ou = YO + (size_t)n * N, *ov = YO + SN + (size_t)n * N;
         const double kp2 = a.kp2[n];
         const bool haveH = (PASS == 1) || (PASS == 3) || (PASS == 0 && !a.fk_given);
         /* bulk L2 prefetch: this state's ABM inputs (used after the FFT phase) and the next
@@ -516,7 +520,9 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
                 if (comp) HV[o] = r; else HU[o] = r;
             }
         }
-        const double c = 1.0 / sqrt(block_sum(nrm, red) * WTD_DV);
+        const double nrm_tot = sqrt(block_sum(nrm, red) * WTD_DV);
+        const double c = 1.0 / nrm_tot;
+        if (a.nrm_out && threadIdx.x == 0) a.nrm_out[n] = nrm_tot;
         /* ---- normalise, store, densities ---- */
         const double f = a.occ[n], w = a.wcnt[n];
         for (int p = threadIdx.x; p < N; p += blockDim.x) {
@@ -525,7 +531,7 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
             double2 u = make_double2((double)hu.x * c, (double)hu.y * c);
             double2 v = make_double2((double)hv.x * c, (double)hv.y * c);
             TY su = from_d<TY>(u), sv = from_d<TY>(v);
-            st_stream(yu + p, su); st_stream(yv + p, sv);
+            st_stream(ou + p, su); st_stream(ov + p, sv);
             u = to_d(su); v = to_d(sv);
             dens_limited(ds, p, N, u, v, f, w, pol);
             if (GRAD) {
@@ -538,8 +544,8 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
             /* const mass: (HU, HV) = (BU, BV) hold the state, B2 is work.
              * variable mass: (HU, HV) = (B2, B3), BU is work. */
             C *Wk = VAR ? BU : B2;
-            dens_gradients<G, TY, TC>(ds, yu, HU, Wk, tw, kt, f, w, kp2, 0);
-            dens_gradients<G, TY, TC>(ds, yv, HV, Wk, tw, kt, f, w, kp2, 1);
+            dens_gradients<G, TY, TC>(ds, ou, HU, Wk, tw, kt, f, w, kp2, 0);
+            dens_gradients<G, TY, TC>(ds, ov, HV, Wk, tw, kt, f, w, kp2, 1);
         }
         __syncthreads();
     }

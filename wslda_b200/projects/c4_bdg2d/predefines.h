@@ -15,6 +15,8 @@
 #define DENSEPSILON 1.0e-8
 #define REGULARIZATION_SCHEME SPHERICAL_CUTOFF
 #define INTEGRATION_SCHEME AB3AM4
+/* Delta = -params[14]*nu, V_a = V_b = v_ext: the adjoint (wtd_adjoint) applies */
+#define WTD_ADJOINT_CONTACT_BDG 14
 
 #include "machine.h"
 #define API_VERSION 20240131
