@@ -40,6 +40,11 @@ WORKLOADS = {
 }
 
 
+# DRAM bytes (read + write) per state of the FP64 passes, from one ncu capture of the same
+# kernel on the same lattice (profiles/wtd_fused_pass_c2_slda2d_64x64.md: 1024 states, pass A
+# 1203 MB, pass B 437 MB); traffic per launch scales with the states processed
+TRAFFIC_PER_STATE = {"c2_slda2d": {"pass_a": 1203152896 / 1024, "pass_b": 436638720 / 1024}}
+
 # bounded CPU samples of each workload (states, steps): about 10-30 s on the host cores
 CPU_SAMPLE = {"c2": (1024, 40), "c1": (256, 4000), "c4": (1024, 60)}
 
@@ -364,7 +369,9 @@ def main():
         "roofline": {"bound": "hbm", "kernel": "wtd_fused_pass<PASS=0> (H psi + ABM predictor)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-                     "traffic": None, "alg_bytes_per_launch": ba * nwf,
+                     "traffic": (TRAFFIC_PER_STATE[proj.name]["pass_a"] * nwf if proj.name in TRAFFIC_PER_STATE else None),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 1024-state capture, scaled by states",
+                     "alg_bytes_per_launch": ba * nwf,
                      "pass_b": {"achieved": bb * nwf / (f["ms_b"] * 1e-3) / 1e9, "alg_bytes_per_launch": bb * nwf},
                      "ms_pass_a": f["ms_a"], "ms_pass_b": f["ms_b"]},
         "clocks": f["clocks"],
