@@ -72,6 +72,11 @@ int compute_gradient_real_f(double *f, double *df_dx, double *df_dy, double *df_
 int compute_derivative_real_vector_f(double *fx, double *fy, double *fz, double *dfx_dx, double *dfy_dy, double *dfz_dz, int nthreads);
 int compute_laplace_real_f(double *f, double *laplace_f, int nthreads);
 int compute_divergence_real_vector_f(double *fx, double *fy, double *fz, double *divf, int nthreads);
+/* Fermi-Dirac high-k filters, FD(k^2/2; mu, T) in k-space (hpc-engine/pca_derivative.cu:829,
+ * 906, 950); out may alias in */
+int high_frequency_filter_d(double *in, double *out, double fd_mu, double fd_T, int nthreads);
+int high_frequency_filter_c(wtd_z *in, wtd_z *out, double fd_mu, double fd_T, int nthreads);
+int high_frequency_filter_massive_d(int n, double *in, double *out, double fd_mu, double fd_T, int nthreads);
 
 /* densities (hpc-engine/pca_dens.cu:220, cpca_dens.cu:239, ccpca_dens.cu:239) */
 #if WTD_CODEDIM == 3

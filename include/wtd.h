@@ -127,6 +127,13 @@ int wtd_adjoint(wtd_ctx *ctx, int it0, int nsteps, int checkpoint_every, const d
                 double *loss, double *grad);
 int wtd_adjoint_release(wtd_ctx *ctx);
 
+/* high-k filter of the effective masses alpha_a, alpha_b after every functional evaluation:
+ * alpha -> IFFT[FD(k^2/2; mu, T) FFT alpha], as the reference's driver with hkf_mode >= 1
+ * (pca.c:1448-1453; high_frequency_filter_massive_d, pca_derivative.cu:950).  mu and T are
+ * energies (the reference's input gives them in units of E_max = pi^2 / (2 dx^2), pca.c:183-185).
+ * Like the reference, it acts in variable-mass builds only; mode 0 turns it off. */
+int wtd_set_high_k_filter(wtd_ctx *ctx, int mode, double mu, double T);
+
 /* ---- state-sharded runs (one process per GPU, each context holding a block of the states) ----
  * Densities are sums over states, so every density reduction of a sharded run is followed by a
  * sum over ranks: the reference's MPI_Allreduce of d_densities (hpc-engine/pca.c:948, 1433,

@@ -87,6 +87,16 @@ extern "C" int refh_nhist(void) { return nhist_of_scheme(); }
  * quasiparticle energies (nwf), history slots f1..fq in the reference's order after the last
  * pointer rotation (q x 2*nwf*N complex), and the device time per step in ms.
  */
+/* effective-mass filtering of the reference driver (pca.c:1448-1453), off unless set */
+static int hkf_mode = 0;
+static double hkf_mu = 0.0, hkf_T = 1.0;
+extern "C" int high_frequency_filter_massive_d(int n, double *in, double *out, double fd_mu, double fd_T, int nthreads);
+extern "C" int refh_set_hkf(int mode, double mu, double T)
+{
+    hkf_mode = mode; hkf_mu = mu; hkf_T = T;
+    return 0;
+}
+
 extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const double *fb,
                         const double *kky, const double *kkz, const int *cnt,
                         double mu_a, double mu_b, double ec, double t0, double dt, double kF, double sclgth,
@@ -195,6 +205,7 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
             if (grads) CK(density_caculate_tau(d_dens, nthreads));
             CK(compute_potentials(it + 1, d_dens, d_pots, 1.0, nthreads));
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+            if (hkf_mode >= 1) CK(high_frequency_filter_massive_d(2, d_pots + 4 * (size_t)RN, d_pots + 4 * (size_t)RN, hkf_mu, hkf_T, nthreads));
             CK(multiply_wf_by_alpha(nwf, d_wf, d_alap, d_pots, nthreads));
             CK(compute_laplace(2 * nwf, d_alap, d_alap, nthreads));
 #endif
@@ -211,6 +222,7 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
             if (grads) CK(density_caculate_tau(d_dens, nthreads));
             CK(compute_potentials(it + 1, d_dens, d_pots, 1.0, nthreads));
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+            if (hkf_mode >= 1) CK(high_frequency_filter_massive_d(2, d_pots + 4 * (size_t)RN, d_pots + 4 * (size_t)RN, hkf_mu, hkf_T, nthreads));
             CK(multiply_wf_by_alpha(nwf, d_wf, d_alap, d_pots, nthreads));
             CK(compute_laplace(2 * nwf, d_alap, d_alap, nthreads));
 #endif

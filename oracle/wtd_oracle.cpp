@@ -200,6 +200,26 @@ static void lap_real(const double *f, double *out)
     derivs_one(F.data(), nullptr, nullptr, nullptr, L.data());
     for (int i = 0; i < N; i++) out[i] = L[i].real();
 }
+/* high_frequency_filter_d (pca_derivative.cu:784-859; cpca_derivative.cu:709-736;
+ * ccpca_derivative.cu:640-662): f -> IFFT[FD(k^2/2) FFT f] / N with FD(e) = 1/(exp((e-mu)/T)+1),
+ * k of index i as kval (the Nyquist mode counted with k = -pi/dx) */
+static int hkf_mode = 0;
+static double hkf_mu = 0.0, hkf_T = 1.0;
+static void high_k_filter(double *f)
+{
+    std::vector<Complex> F(N);
+    for (int i = 0; i < N; i++) F[i] = Complex(f[i], 0.0);
+    fftn(F.data(), -1);
+    for (int i = 0; i < N; i++) {
+        int c[3]; decode(i, c[0], c[1], c[2]);
+        double k2 = 0.0;
+        for (int d = 0; d < CODEDIM; d++) { double k = kval(d, c[d]); k2 += k * k; }
+        const double w = 1.0 / (std::exp((0.5 * k2 - hkf_mu) / hkf_T) + 1.0) / N;
+        F[i] *= w;
+    }
+    fftn(F.data(), +1);
+    for (int i = 0; i < N; i++) f[i] = F[i].real();
+}
 static void dcomp_real(const double *f, int d, double *out)
 {
     std::vector<Complex> F(N), D(N);
@@ -681,6 +701,13 @@ static void half_step_densities(int it_next, int grads)
     exchange_densities();
     if (grads) density_tau();
     compute_potentials(it_next);
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+    if (hkf_mode >= 1) { /* effective-mass filtering (pca.c:1448-1453) */
+        wslda_potential P = pots_view(pots.data());
+        high_k_filter(P.alpha_a);
+        high_k_filter(P.alpha_b);
+    }
+#endif
     alpha_laplace(y);
 }
 
@@ -875,6 +902,17 @@ int orc_get_history(int slot, double *out)
     return 0;
 }
 int orc_get_it(void) { return it_global; }
+int orc_set_high_k_filter(int mode, double mu, double T)
+{
+    hkf_mode = mode; hkf_mu = mu; hkf_T = T;
+    return 0;
+}
+int orc_filter_field(double *f)
+{
+    for (int d = 0; d < 3; d++) if (plans[d].n != AXN[d]) make_plan(plans[d], AXN[d]);
+    high_k_filter(f);
+    return 0;
+}
 int orc_set_density_exchange(exchange_fn fn, void *user)
 {
     xfn = fn;

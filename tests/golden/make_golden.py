@@ -35,6 +35,22 @@ CASES = {
     "c5_slda3d": (4, 2, 1, False),
 }
 
+# effective-mass filter cases (pca.c:1448-1453, hkf_mode 1): the same runs with alpha_a,
+# alpha_b filtered by FD(k^2/2; mu, T) after every functional evaluation; mu and T as fractions
+# of E_max = pi^2 / (2 dx^2), as the reference's input gives them (pca.c:183-185)
+HKF_CASES = {
+    "t1d_aslda": (24, 3, 2, True),
+    "t3d_aslda": (24, 3, 2, True),
+    "c3_aslda3d": (8, 2, 1, False),
+}
+HKF_FRACTIONS = (0.35, 0.04)
+
+
+def hkf_params(proj):
+    emax = 0.5 * np.pi ** 2 / proj.dx ** 2
+    return 1, HKF_FRACTIONS[0] * emax, HKF_FRACTIONS[1] * emax
+
+
 _dp = ctypes.POINTER(ctypes.c_double)
 
 
@@ -83,11 +99,14 @@ def slim(rec, n):
     return rec
 
 
-def run_case(name, out_dir):
-    nwf, nsteps, nmeas, full = CASES[name]
+def run_case(name, out_dir, hkf=False):
+    nwf, nsteps, nmeas, full = (HKF_CASES if hkf else CASES)[name]
     proj, y0, occ, pots, params, extra = case_inputs(name, nwf)
     so = os.path.join(REPO, "oracle", "_ref", name, "libref.so")
     lib = ctypes.CDLL(so, mode=ctypes.RTLD_LOCAL)
+    lib.refh_set_hkf.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
+    mode, mu, T = hkf_params(proj) if hkf else (0, 0.0, 1.0)
+    lib.refh_set_hkf(mode, mu, T)
     lib.refh_numel.restype = ctypes.c_int
     lib.refh_nhist.restype = ctypes.c_int
     n = lib.refh_numel()
@@ -117,8 +136,10 @@ def run_case(name, out_dir):
     if full:
         rec["states"] = y
         rec["history0"] = hist[:M]
+    if hkf:
+        rec["hkf"] = np.array([mode, mu, T])
     rec = slim(rec, n)
-    path = os.path.join(out_dir, f"{name}.npz")
+    path = os.path.join(out_dir, f"{name}_hkf.npz" if hkf else f"{name}.npz")
     np.savez_compressed(path, **rec)
     print(f"{name}: nwf={nwf} steps={nsteps}x{nmeas} E={en[:7].sum():.12g} N={en[7]:.12g},{en[8]:.12g} "
           f"ms/step={ms[0]:.3f} -> {path}")
@@ -128,6 +149,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--slim-existing", action="store_true", help="apply slim() to fixtures in --out")
+    ap.add_argument("--hkf", action="store_true", help="the effective-mass filter cases (HKF_CASES)")
     ap.add_argument("projects", nargs="*")
     a = ap.parse_args()
     if a.slim_existing:
@@ -140,8 +162,8 @@ def main():
                     np.savez_compressed(path, **slim(rec, n))
         return
     os.makedirs(a.out, exist_ok=True)
-    for name in (a.projects or list(CASES)):
-        run_case(name, a.out)
+    for name in (a.projects or list(HKF_CASES if a.hkf else CASES)):
+        run_case(name, a.out, hkf=a.hkf)
 
 
 if __name__ == "__main__":

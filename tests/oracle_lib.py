@@ -57,7 +57,12 @@ class Oracle:
         L.orc_fft_field.argtypes = [_dp, ctypes.c_int]
         L.orc_derivatives_field.argtypes = [_dp] * 5
         L.orc_set_density_exchange.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_set_high_k_filter.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.orc_filter_field.argtypes = [_dp]
         self._xfn = None
+        # the library is shared by every instance in the process: start from a plain run
+        L.orc_set_high_k_filter(0, 0.0, 1.0)
+        L.orc_set_density_exchange(None, None)
         if threads:
             L.orc_set_threads(int(threads))
         self.N = L.orc_numel()
@@ -80,6 +85,14 @@ class Oracle:
 
     def initial_measurement(self):
         return self.lib.orc_initial_measurement()
+
+    def set_high_k_filter(self, mode, mu, T):
+        self.lib.orc_set_high_k_filter(int(mode), float(mu), float(T))
+
+    def filter_field(self, f):
+        a = np.ascontiguousarray(f, dtype=np.float64).copy()
+        self.lib.orc_filter_field(_p(a))
+        return a
 
     def set_density_exchange(self, fn):
         """fn(dens) with dens a numpy view of the 12N partial densities, summed in place over

@@ -179,3 +179,46 @@ def test_compat_abi_matches_reference_golden(has_gpu, name):
     if "states" in g.files:
         assert rel(o["states"], g["states"]) < TOL
         assert rel(o["history0"], g["history0"]) < TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["t1d_aslda", "t2d_slda", "t3d_aslda", "c3_aslda3d"])
+def test_compat_high_k_filters(has_gpu, name):
+    """high_frequency_filter_{d,massive_d,c} (pca_derivative.cu:829-963) against the oracle's
+    filter, in place and out of place, on the fused-size and the plane/pencil (32^3) lattices"""
+    from oracle_lib import Oracle
+    from wslda_b200 import load_library
+    from wslda_b200.projects import Project
+    proj = Project(name)
+    N = proj.numel
+    lib = load_library(name)
+    for fn in ("gpu_malloc", "gpu_free", "memcopy_host2gpu", "memcopy_gpu2host"):
+        getattr(lib, fn).restype = ctypes.c_int
+    lib.high_frequency_filter_massive_d.argtypes = [ctypes.c_int, VP, VP, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    lib.high_frequency_filter_d.argtypes = [VP, VP, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    lib.high_frequency_filter_c.argtypes = [VP, VP, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    emax = 0.5 * np.pi ** 2 / proj.dx ** 2
+    mu, T = 0.35 * emax, 0.04 * emax
+    o = Oracle(name)
+    o.set_high_k_filter(1, mu, T)
+    rng = np.random.default_rng(11)
+    f = rng.standard_normal((3, N))
+    want = np.stack([o.filter_field(f[k]) for k in range(3)])
+    src, dst = Dev(lib, f.nbytes), Dev(lib, f.nbytes)
+    src.put(f)
+    assert lib.high_frequency_filter_massive_d(3, src.p, dst.p, mu, T, 512) == 0
+    got = dst.get(np.float64, 3 * N).reshape(3, N)
+    assert np.max(np.abs(got - want)) < 1e-12 * np.max(np.abs(f))
+    assert np.array_equal(src.get(np.float64, 3 * N).reshape(3, N), f)  # input untouched
+    assert lib.high_frequency_filter_d(src.p, src.p, mu, T, 512) == 0  # in place, first field
+    assert np.max(np.abs(src.get(np.float64, N) - want[0])) < 1e-12 * np.max(np.abs(f))
+    # complex field: the filter is real and even in k, so it acts on Re and Im separately
+    z = f[1] + 1j * f[2]
+    zs, zd = Dev(lib, z.nbytes), Dev(lib, z.nbytes)
+    zs.put(z)
+    assert lib.high_frequency_filter_c(zs.p, zd.p, mu, T, 512) == 0
+    zg = zd.get(np.complex128, N)
+    assert np.max(np.abs(zg - (want[1] + 1j * want[2]))) < 1e-12 * np.max(np.abs(f))
+    o.set_high_k_filter(0, 0.0, 1.0)
+    for x in (src, dst, zs, zd):
+        x.free()

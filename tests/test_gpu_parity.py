@@ -14,9 +14,9 @@ TOL = 1e-10
 SMALL = ["t1d_custom", "t1d_aslda", "t2d_slda", "t2d_bdg", "t3d_slda", "t3d_aslda"]
 
 
-def _compare(name, nwf, nsteps, nmeas, tol=TOL):
-    o = run_oracle(name, nwf, nsteps, nmeas)
-    g = run_gpu(name, nwf, nsteps, nmeas)
+def _compare(name, nwf, nsteps, nmeas, tol=TOL, hkf=None):
+    o = run_oracle(name, nwf, nsteps, nmeas, hkf=hkf)
+    g = run_gpu(name, nwf, nsteps, nmeas, hkf=hkf)
     n = o["densities"].size // 12
     errs = density_errors(g["densities"], o["densities"], n)
     for k, v in errs.items():
@@ -65,3 +65,15 @@ def test_c3_aslda3d_small_s(has_gpu):
 def test_c5_slda3d_small_s(has_gpu):
     """3D SLDA 48^3 (radix-3 axes) through the staged path."""
     _compare("c5_slda3d", nwf=4, nsteps=2, nmeas=1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,nwf,nsteps", [("t1d_aslda", 24, 3), ("t3d_aslda", 24, 3), ("c3_aslda3d", 8, 2)])
+def test_high_k_filter_of_masses(has_gpu, name, nwf, nsteps):
+    """variable-mass runs with the effective-mass filter (pca.c:1448-1453) on: fused path
+    (t1d, t3d) and staged plane/pencil path (c3, 32^3)"""
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from golden.make_golden import hkf_params
+    from wslda_b200.projects import Project
+    _compare(name, nwf=nwf, nsteps=nsteps, nmeas=2 if nsteps == 3 else 1, hkf=hkf_params(Project(name)))

@@ -58,3 +58,35 @@ def test_step_keeps_states_normalised(name):
     # particle number: sum of rho over the lattice, times dV, equals the energy slots 7, 8
     assert abs(dens[2 * n:3 * n].sum() * {1: proj.dx, 2: proj.dx * proj.dy, 3: proj.dv}[proj.codedim] - e[7]) < 1e-10 * max(1, abs(e[7]))
     assert o.lib.orc_get_it() == 3
+
+
+@pytest.mark.parametrize("project", ["t1d_aslda", "t2d_slda", "t3d_aslda"])
+def test_oracle_high_k_filter_matches_numpy(project):
+    """the oracle's Fermi-Dirac filter (high_frequency_filter_d) against numpy's FFT"""
+    from oracle_lib import Oracle
+    from wslda_b200.projects import Project
+    proj = Project(project)
+    o = Oracle(project)
+    dims = proj.dims[:proj.codedim]
+    spacing = [proj.dx, proj.dy, proj.dz][:proj.codedim]
+    rng = np.random.default_rng(7)
+    f = rng.standard_normal(proj.numel)
+    emax = 0.5 * np.pi ** 2 / proj.dx ** 2
+    mu, T = 0.35 * emax, 0.04 * emax
+    o.set_high_k_filter(1, mu, T)
+    got = o.filter_field(f)
+    o.set_high_k_filter(0, 0.0, 1.0)
+    ks = [2 * np.pi * np.fft.fftfreq(n, d=h) for n, h in zip(dims, spacing)]
+    # the reference counts the Nyquist mode as -pi/dx; k^2 is the same either way
+    grids = np.meshgrid(*ks, indexing="ij")
+    ek = 0.5 * sum(k ** 2 for k in grids)
+    w = 1.0 / (np.exp((ek - mu) / T) + 1.0)
+    want = np.fft.ifftn(np.fft.fftn(f.reshape(dims)) * w).real.reshape(-1)
+    assert np.max(np.abs(got - want)) < 1e-12 * np.max(np.abs(f))
+    # a very high cut-off keeps the field, a constant keeps FD(0) of itself
+    o.set_high_k_filter(1, 1e6 * emax, 1e-3 * emax)
+    assert np.allclose(o.filter_field(f), f, rtol=0, atol=1e-12)
+    o.set_high_k_filter(1, mu, T)
+    c = o.filter_field(np.full(proj.numel, 2.0))
+    assert np.allclose(c, 2.0 / (np.exp(-mu / T) + 1.0), rtol=1e-13)
+    o.set_high_k_filter(0, 0.0, 1.0)

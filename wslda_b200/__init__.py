@@ -53,6 +53,7 @@ SIGNATURES = {
     "wtd_pass_times": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _ip, _ip]),
     "wtd_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp]),
     "wtd_adjoint_release": (ctypes.c_int, [ctypes.c_void_p]),
+    "wtd_set_high_k_filter": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double]),
     "wtd_nccl_unique_id": (ctypes.c_int, [ctypes.c_void_p]),
     "wtd_nccl_attach": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "wtd_set_density_exchange": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
@@ -223,6 +224,11 @@ class TDRun:
 
         self._xfn = EXCHANGE_FN(tramp)
         self._check(self.lib.wtd_set_density_exchange(self.h, ctypes.cast(self._xfn, ctypes.c_void_p), None))
+
+    def set_high_k_filter(self, mode, mu, T):
+        """Fermi-Dirac filter of alpha_a, alpha_b after each functional evaluation (variable
+        mass); mu, T are energies"""
+        self._check(self.lib.wtd_set_high_k_filter(self.h, int(mode), float(mu), float(T)))
 
     def adjoint_release(self):
         """free the adjoint's device workspace (kept between gradient calls)"""

@@ -50,6 +50,9 @@ struct wtd_ctx {
     void *xuser;
     /* adjoint workspace kept between gradient calls (AdjWork, released with the context) */
     void *adj;
+    /* high-k filter of the effective masses after every functional evaluation (variable mass) */
+    int hkf_mode;
+    double hkf_mu, hkf_T;
 };
 
 static void adj_release(wtd_ctx *c);
@@ -192,6 +195,23 @@ static int ensure_fk(wtd_ctx *c)
     return WTD_OK;
 }
 
+/* high-k filter of alpha_a and alpha_b after the functional (hkf_mode >= 1), as the
+ * reference's driver does for variable-mass runs (pca.c:1448-1453, cpca.c:1014-1017) */
+static int filter_masses(wtd_ctx *c)
+{
+    if (c->hkf_mode < 1) return WTD_OK;
+    constexpr size_t N = WTD_NUMEL;
+    double *alpha = c->pots + 4 * N; /* alpha_a, alpha_b consecutive */
+    if (WTD_BIG) return big_filter_real(alpha, 2, c->hkf_mu, c->hkf_T, c->stage3d, c->tw, c->ktab, c->st);
+    constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
+    if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+    static bool attr = false;
+    if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_hkf_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+    wtd_hkf_kernel<WG><<<2, 512, sm, c->st>>>(alpha, c->hkf_mu, c->hkf_T, c->tw, c->ktab);
+    WTD_LAUNCHED(c);
+    return WTD_OK;
+}
+
 /* densities from the slots, tau, potentials and H coefficients at time index it */
 static int after_pass(wtd_ctx *c, bool full, int it)
 {
@@ -217,6 +237,9 @@ static int after_pass(wtd_ctx *c, bool full, int it)
 #ifdef ENABLE_MODIFY_POTENTIALS
     modify_potentials<<<pb, 128, 0, c->st>>>(it, D, P);
     WTD_LAUNCHED(c);
+#endif
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+    WTD_TRY(filter_masses(c));
 #endif
     wtd_prep_coef<<<pb, 128, 0, c->st>>>(it, P, c->cf);
     WTD_LAUNCHED(c);
@@ -273,6 +296,9 @@ static int staged_potentials(wtd_ctx *c, int it)
 #ifdef ENABLE_MODIFY_POTENTIALS
     modify_potentials<<<pb, 128, 0, c->st>>>(it, D, P);
     WTD_LAUNCHED(c);
+#endif
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+    WTD_TRY(filter_masses(c));
 #endif
     wtd_prep_coef<<<pb, 128, 0, c->st>>>(it, P, c->cf);
     WTD_LAUNCHED(c);
@@ -400,16 +426,18 @@ static int fused_step(wtd_ctx *c, bool last, StepRecord *rec, double2 *yk_next =
 template <typename TY, typename TH, typename TC>
 static int occupancy_t(int block)
 {
-    constexpr int NBUF = WTD_VAR ? 4 : 3;
+    /* resident CTAs of the step's ordinary passes (PASS 0 without gradients); the gradient
+     * passes (one more buffer) may then run the same grid in more than one wave */
+    constexpr int NBUF = WTD_VAR ? 4 : 2;
     constexpr size_t sm = fused_smem<TC, NBUF>();
     if (sm > WTD_SMEM_MAX) return 1;
     int nb = 1;
     if (block == 1024 && WG::ntot >= 2048) {
-        auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, 1, WTD_VAR, true, 1024>;
+        auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, 0, WTD_VAR, false, 1024>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 1024, sm);
     } else {
-        auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, 1, WTD_VAR, true, 512>;
+        auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, 0, WTD_VAR, false, 512>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         int threads = WG::ntot >= 512 ? 512 : ((WG::ntot + 31) / 32) * 32;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, sm);
@@ -483,11 +511,11 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
         const char *b = getenv("WTD_BLOCK");
         if (b && atoi(b) == 1024) c->block = 1024;
     }
-    /* persistent grid: as many CTAs as fit on every SM for the most demanding pass variant
-     * (the gradient pass), so all variants of a run share one slot layout */
-    /* L2 prefetch of the next state's y only for FP64 (prefetching the FP64 history as well
-     * overflows L2 with 148 states in flight and is re-read from HBM); FP32 forms prefetch both */
-    c->prefetch = (precision == WTD_FP64) ? 1 : 3;
+    /* persistent grid: as many CTAs as fit on every SM for the step's ordinary passes (two per
+     * SM for the FP32 compute forms), one slot layout for all pass variants of a run */
+    /* L2 prefetch of the next state's y only: prefetching the history as well overflows L2
+     * with one FP64 or two FP32 CTAs per SM in flight and is re-read from HBM */
+    c->prefetch = 1;
     {
         const char *pf = getenv("WTD_PREFETCH");
         if (pf) c->prefetch = atoi(pf) & 3;
@@ -890,6 +918,15 @@ int wtd_nccl_attach(wtd_ctx *c, const void *id128, int nranks, int rank)
     ncclComm_t comm = NULL;
     if (a->comm_init_rank(&comm, nranks, id, rank) != ncclSuccess) return WTD_ERR_COMM;
     c->nccl = comm;
+    return WTD_OK;
+}
+
+int wtd_set_high_k_filter(wtd_ctx *c, int mode, double mu, double T)
+{
+    if (!c || (mode >= 1 && !(T > 0.0))) return WTD_ERR_ARG;
+    c->hkf_mode = mode;
+    c->hkf_mu = mu;
+    c->hkf_T = T;
     return WTD_OK;
 }
 

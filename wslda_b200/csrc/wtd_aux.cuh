@@ -133,6 +133,72 @@ __global__ void __launch_bounds__(256) wtd_prep_var(double *cf, const double2 *g
         cf[(s == 0 ? CF_CJA : CF_CJB) * (size_t)N + p] = -0.5 * acc[k];
 }
 
+/* Fermi-Dirac high-k filter of real fields (high_frequency_filter_d, pca_derivative.cu:784-859;
+ * 2D cpca_derivative.cu:709-736, 1D ccpca_derivative.cu:640-662): f -> IFFT[FD(k^2/2) FFT f],
+ * FD(e) = 1 / (exp((e - mu) / T) + 1), the Nyquist mode counted with |k| = pi/dx.
+ * blockIdx.x = field (consecutive fields of N doubles, filtered in place). */
+template <class G>
+__global__ void __launch_bounds__(512) wtd_hkf_kernel(double *f, double mu, double T, const double2 *gtw, const double *gk)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *B = (double2 *)smem_raw;
+    double2 *tw = B + G::padded;
+    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    load_tables<G>(tw, kt, gtw, gk);
+    constexpr int N = G::ntot;
+    double *a = f + (size_t)blockIdx.x * N;
+    field_to_smem<G>(B, a);
+    fft_forward<G, 1>(B, 0, tw);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        int c0, c1 = 0, c2 = 0;
+        if (G::dims == 1) { c0 = i; }
+        else if (G::dims == 2) { c0 = i / G::N1; c1 = i - c0 * G::N1; }
+        else { c0 = i / (G::N1 * G::N2); int r = i - c0 * G::N1 * G::N2; c1 = r / G::N2; c2 = r - c1 * G::N2; }
+        double k2 = kt[0][c0] * kt[0][c0];
+        if (G::dims >= 2) k2 += kt[1][c1] * kt[1][c1];
+        if (G::dims >= 3) k2 += kt[2][c2] * kt[2][c2];
+        const double w = 1.0 / (exp((0.5 * k2 - mu) / T) + 1.0) / N;
+        const int o = G::off(i);
+        B[o].x *= w;
+        B[o].y *= w;
+    }
+    __syncthreads();
+    fft_inverse<G, 1>(B, 0, tw);
+    for (int p = threadIdx.x; p < N; p += blockDim.x) a[p] = B[G::off(p)].x;
+}
+
+/* the same filter of complex fields (high_frequency_filter_c, pca_derivative.cu:861-935) */
+template <class G>
+__global__ void __launch_bounds__(512) wtd_hkf_c_kernel(const double2 *in, double2 *out, double mu, double T,
+                                                        const double2 *gtw, const double *gk)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *B = (double2 *)smem_raw;
+    double2 *tw = B + G::padded;
+    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    load_tables<G>(tw, kt, gtw, gk);
+    constexpr int N = G::ntot;
+    for (int p = threadIdx.x; p < N; p += blockDim.x) B[G::off(p)] = in[p];
+    __syncthreads();
+    fft_forward<G, 1>(B, 0, tw);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        int c0, c1 = 0, c2 = 0;
+        if (G::dims == 1) { c0 = i; }
+        else if (G::dims == 2) { c0 = i / G::N1; c1 = i - c0 * G::N1; }
+        else { c0 = i / (G::N1 * G::N2); int r = i - c0 * G::N1 * G::N2; c1 = r / G::N2; c2 = r - c1 * G::N2; }
+        double k2 = kt[0][c0] * kt[0][c0];
+        if (G::dims >= 2) k2 += kt[1][c1] * kt[1][c1];
+        if (G::dims >= 3) k2 += kt[2][c2] * kt[2][c2];
+        const double w = 1.0 / (exp((0.5 * k2 - mu) / T) + 1.0) / N;
+        const int o = G::off(i);
+        B[o].x *= w;
+        B[o].y *= w;
+    }
+    __syncthreads();
+    fft_inverse<G, 1>(B, 0, tw);
+    for (int p = threadIdx.x; p < N; p += blockDim.x) out[p] = B[G::off(p)];
+}
+
 /* sum of each of the TDWSLDAITEMS integrand arrays (one CTA per item) */
 __global__ void wtd_sum_items(const double *e, int N, double *out, double volel)
 {

@@ -293,6 +293,13 @@ __global__ void k_overlap(int n, const double2 *a, const double2 *b, double *re,
     }
 }
 
+/* out += a (+ b) */
+__global__ void k_add_fields(double *out, const double *a, const double *b, int n)
+{
+    int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i < n) out[i] += a[i] + (b ? b[i] : 0.0);
+}
+
 __global__ void k_get_vext(int it, int spin, double *out)
 {
     int i = threadIdx.x + blockIdx.x * blockDim.x;
@@ -663,15 +670,51 @@ int compute_divergence_real_vector_f(double *fx, double *fy, double *fz, double 
     int r = compat_real_deriv(fx, divf, 1);
     if (!r && CODEDIM >= 2) { r = compat_real_deriv(fy, t, 2); }
     if (!r && CODEDIM >= 3) { r = compat_real_deriv(fz, t + WTD_NUMEL, 3); }
-    if (!r) {
-        std::vector<double> a(WTD_NUMEL), b(2 * WTD_NUMEL);
-        cudaMemcpy(a.data(), divf, sizeof(double) * WTD_NUMEL, cudaMemcpyDeviceToHost);
-        cudaMemcpy(b.data(), t, 2 * sizeof(double) * WTD_NUMEL, cudaMemcpyDeviceToHost);
-        for (int i = 0; i < WTD_NUMEL; i++) a[i] += (CODEDIM >= 2 ? b[i] : 0.0) + (CODEDIM >= 3 ? b[WTD_NUMEL + i] : 0.0);
-        cudaMemcpy(divf, a.data(), sizeof(double) * WTD_NUMEL, cudaMemcpyHostToDevice);
+    if (!r && CODEDIM >= 2) {
+        k_add_fields<<<(WTD_NUMEL + 255) / 256, 256>>>(divf, t, CODEDIM >= 3 ? t + WTD_NUMEL : NULL, WTD_NUMEL);
+        r = cu_sync_status();
     }
     cudaFree(t);
     return r;
+}
+
+/* high-k filters (pca_derivative.cu:829-859, 906-935, 950-963): in -> IFFT[FD(k^2/2) FFT in];
+ * out may alias in */
+int high_frequency_filter_massive_d(int n, double *in, double *out, double fd_mu, double fd_T, int nthreads)
+{
+    if (n < 0 || !(fd_T > 0.0)) return WTD_ERR_ARG;
+    if (n == 0) return 0;
+    int r = compat_tables();
+    if (r) return r;
+    if (out != in) cudaMemcpy(out, in, (size_t)n * WTD_NUMEL * sizeof(double), cudaMemcpyDeviceToDevice);
+    if (WTD_BIG) {
+        WTD_TRY(compat_stage());
+        WTD_TRY(big_filter_real(out, n, fd_mu, fd_T, g_stage3d, g_tw, g_ktab, 0));
+        return cu_sync_status();
+    }
+    if (k_field_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+    cudaFuncSetAttribute(wtd_hkf_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k_field_smem);
+    wtd_hkf_kernel<WG><<<n, 512, k_field_smem>>>(out, fd_mu, fd_T, g_tw, g_ktab);
+    return cu_sync_status();
+}
+int high_frequency_filter_d(double *in, double *out, double fd_mu, double fd_T, int nthreads)
+{
+    return high_frequency_filter_massive_d(1, in, out, fd_mu, fd_T, nthreads);
+}
+int high_frequency_filter_c(wtd_z *in, wtd_z *out, double fd_mu, double fd_T, int nthreads)
+{
+    if (!(fd_T > 0.0)) return WTD_ERR_ARG;
+    int r = compat_tables();
+    if (r) return r;
+    if (WTD_BIG) {
+        WTD_TRY(compat_stage());
+        WTD_TRY(big_derivs((double2 *)in, 1, (double2 *)out, NULL, NULL, NULL, g_tw, g_ktab, 0, 1, fd_mu, fd_T));
+        return cu_sync_status();
+    }
+    if (k_field_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+    cudaFuncSetAttribute(wtd_hkf_c_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k_field_smem);
+    wtd_hkf_c_kernel<WG><<<1, 512, k_field_smem>>>((const double2 *)in, (double2 *)out, fd_mu, fd_T, g_tw, g_ktab);
+    return cu_sync_status();
 }
 
 static int calculate_densities_impl(int n, wtd_z *wf, wtd_z *dx, wtd_z *dy, wtd_z *dz, wtd_z *lap, const double *kky,

@@ -45,7 +45,8 @@ __global__ void __launch_bounds__(512) k_planes(const double2 *in, double2 *out,
  * ops bit 0: laplacian, bit 1..3: d/dx, d/dy, d/dz.  Outputs may alias the input. */
 template <class GX>
 __global__ void __launch_bounds__(512) k_pencils(const double2 *in, double2 *olap, double2 *odx, double2 *ody, double2 *odz,
-                                                 int nyz, int N, const double2 *gtw_x, const double *gk)
+                                                 int nyz, int N, const double2 *gtw_x, const double *gk,
+                                                 int filt, double fmu, double fT)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *B0 = (double2 *)smem_raw;
@@ -77,8 +78,10 @@ __global__ void __launch_bounds__(512) k_pencils(const double2 *in, double2 *ola
             double2 z = B0[GX::off(x * PX + j)];
             double2 r;
             if (op == 0) {
+                /* laplacian -|k|^2/N, or (filt) the high-k filter FD(|k|^2/2)/N into olap */
                 double kx = kt[0][x], ky = kt[1][yq], kz = kt[2][zq];
-                double s = -1.0 * (kx * kx + ky * ky + kz * kz) / (double)N;
+                double k2 = kx * kx + ky * ky + kz * kz;
+                double s = filt ? 1.0 / (exp((0.5 * k2 - fmu) / fT) + 1.0) / (double)N : -1.0 * k2 / (double)N;
                 r = make_double2(z.x * s, z.y * s);
             } else {
                 double k = (op == 1) ? kt[3][x] : (op == 2) ? kt[4][yq] : kt[5][zq];
@@ -106,7 +109,8 @@ static constexpr size_t pencils_smem = 2 * (size_t)WGX::padded * sizeof(double2)
 /* twiddles of the plane geometry start at the y axis of the lattice table (offset NX) and of
  * the pencil geometry at the x axis (offset 0): both are e^{-2 pi i t/n} per axis */
 static int big_derivs(double2 *in, int nf, double2 *lap, double2 *dx, double2 *dy, double2 *dz,
-                      const double2 *tw, const double *ktab, cudaStream_t st)
+                      const double2 *tw, const double *ktab, cudaStream_t st, int filt = 0, double fmu = 0.0,
+                      double fT = 1.0)
 {
     constexpr int NYZ = NY * NZ, N = NX * NY * NZ;
     if (NYZ % WTD_PX != 0) return WTD_ERR_UNSUPPORTED;
@@ -122,7 +126,7 @@ static int big_derivs(double2 *in, int nf, double2 *lap, double2 *dx, double2 *d
      * overwritten by its transform) */
     double2 *K = lap ? lap : in;
     k_planes<WGP, -1><<<nf * NX, 512, planes_smem, st>>>(in, K, NX, tw + NX, ktab);
-    k_pencils<WGX><<<nf * (NYZ / WTD_PX), 512, pencils_smem, st>>>(K, lap, dx, dy, dz, NYZ, N, tw, ktab);
+    k_pencils<WGX><<<nf * (NYZ / WTD_PX), 512, pencils_smem, st>>>(K, lap, dx, dy, dz, NYZ, N, tw, ktab, filt, fmu, fT);
     double2 *outs[4] = {lap, dx, dy, dz};
     for (int k = 0; k < 4; k++)
         if (outs[k]) k_planes<WGP, +1><<<nf * NX, 512, planes_smem, st>>>(outs[k], outs[k], NX, tw + NX, ktab);
@@ -166,6 +170,21 @@ static int big_real_deriv(const double *f, double *out, int which, double scale,
     }
     if (r) return r;
     k_c_to_real<<<nb, 256, 0, st>>>(res, out, N, scale, accumulate);
+    return cudaGetLastError() == cudaSuccess ? WTD_OK : WTD_ERR_CUDA;
+}
+
+/* high-k filter of nf consecutive real fields of N doubles, in place (large lattices);
+ * stage holds N complex numbers of scratch */
+static int big_filter_real(double *f, int nf, double mu, double T, double2 *stage, const double2 *tw, const double *kt,
+                           cudaStream_t st)
+{
+    constexpr int N = NX * NY * NZ;
+    const int nb = (N + 255) / 256;
+    for (int k = 0; k < nf; k++) {
+        k_real_to_c<<<nb, 256, 0, st>>>(f + (size_t)k * N, stage, N);
+        WTD_TRY(big_derivs(stage, 1, stage, NULL, NULL, NULL, tw, kt, st, 1, mu, T));
+        k_c_to_real<<<nb, 256, 0, st>>>(stage, f + (size_t)k * N, N, 1.0, 0);
+    }
     return cudaGetLastError() == cudaSuccess ? WTD_OK : WTD_ERR_CUDA;
 }
 

@@ -375,7 +375,7 @@ __device__ __forceinline__ void dens_gradients(double *ds, const TY *ysrc, typen
  * VAR: variable effective mass; GRAD: tau and j of the output state too.
  * -------------------------------------------------------------------------------------*/
 template <class G, typename TY, typename TH, typename TC, int NH, int PASS, bool VAR, bool GRAD, int BS>
-__global__ void __launch_bounds__(BS, 1)
+__global__ void __launch_bounds__(BS, (sizeof(TC) == 4 && BS == 512) ? 2 : 1) /* FP32 compute: 2 CTAs/SM */
 wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
 {
     typedef typename cplx<TC>::t C;
