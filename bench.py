@@ -1,6 +1,6 @@
 """Throughput of the TD-(A)SLDA/BdG step on B200: qp-state*steps/s.
 
-Workload (BASELINE configs[1]): 2D TD-SLDA, 64x64 lattice (dx=1, periodic), 8192 (u, v) states,
+Workload: 2D TD-SLDA, 64x64 lattice (dx=1, periodic), 8192 (u, v) states,
 seeded Gaussian QR-orthonormalised, harmonic trap omega=0.04, vortex Delta_ext, AB5AM5, FP64.
 A step is one full ABM predictor-corrector step of every state (both stream passes, both
 density reductions and both functional evaluations).

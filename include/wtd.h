@@ -127,11 +127,13 @@ int wtd_adjoint(wtd_ctx *ctx, int it0, int nsteps, int checkpoint_every, const d
                 double *loss, double *grad);
 int wtd_adjoint_release(wtd_ctx *ctx);
 
-/* high-k filter of the effective masses alpha_a, alpha_b after every functional evaluation:
- * alpha -> IFFT[FD(k^2/2; mu, T) FFT alpha], as the reference's driver with hkf_mode >= 1
- * (pca.c:1448-1453; high_frequency_filter_massive_d, pca_derivative.cu:950).  mu and T are
- * energies (the reference's input gives them in units of E_max = pi^2 / (2 dx^2), pca.c:183-185).
- * Like the reference, it acts in variable-mass builds only; mode 0 turns it off. */
+/* high-k filters of the fields H is built from, f -> IFFT[FD(k^2/2; mu, T) FFT f], in place
+ * after every functional evaluation, as the reference's driver and apply_hamiltonian do
+ * (hkf_mode, pca_utils.h:131-133): mode >= 1 filters V_a, V_b (pca_kernels.cu:700-704), the
+ * effective masses in variable-mass builds (pca.c:1448-1453) and the A components with
+ * current corrections outside BdG (pca_kernels.cu:791-795); mode >= 2 also the pairing field
+ * (pca_kernels.cu:758-762).  mu and T are energies (the reference's input gives them in units
+ * of E_max = pi^2 / (2 dx^2), pca.c:183-185); mode 0 turns filtering off. */
 int wtd_set_high_k_filter(wtd_ctx *ctx, int mode, double mu, double T);
 
 /* ---- state-sharded runs (one process per GPU, each context holding a block of the states) ----

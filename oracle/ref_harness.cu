@@ -113,6 +113,9 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
     md.sclgth = sclgth;
     md.ec = ec;
     md.dt = dt;
+    md.hkf_mode = hkf_mode; /* apply_hamiltonian reads it for the pairing-field filter */
+    md.hkf_mu = hkf_mu;
+    md.hkf_T = hkf_T;
     for (int k = 0; k < MAX_USER_PARAMS; k++) md.params[k] = params[k];
 
     Z *d_wf = alloc_z(M), *d_f[5] = {0, 0, 0, 0, 0};

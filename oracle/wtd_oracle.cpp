@@ -36,6 +36,9 @@ static double dc_params[MAX_USER_PARAMS];
 #else
 #define ORC_U_EXT(ix, iy, iz, it, spin) 0.0
 #endif
+#if defined(ENABLE_VELOCITY_EXT)
+#define ORC_VEL_EXT(ix, iy, iz, it, spin, ax) velocity_ext(ix, iy, iz, it, spin, ax, dc_params, dc_extra_data_size, dc_extra_data)
+#endif
 #if defined(ENABLE_DELTA_EXT)
 #define ORC_D_EXT(ix, iy, iz, it, d) delta_ext(ix, iy, iz, it, d, dc_params, dc_extra_data_size, dc_extra_data)
 #else
@@ -219,6 +222,20 @@ static void high_k_filter(double *f)
     }
     fftn(F.data(), +1);
     for (int i = 0; i < N; i++) f[i] = F[i].real();
+}
+/* high_frequency_filter_c (pca_derivative.cu:861-935): the same filter of a complex field */
+static void high_k_filter_c(Complex *f)
+{
+    std::vector<Complex> F(f, f + N);
+    fftn(F.data(), -1);
+    for (int i = 0; i < N; i++) {
+        int c[3]; decode(i, c[0], c[1], c[2]);
+        double k2 = 0.0;
+        for (int d = 0; d < CODEDIM; d++) { double k = kval(d, c[d]); k2 += k * k; }
+        F[i] *= 1.0 / (std::exp((0.5 * k2 - hkf_mu) / hkf_T) + 1.0) / N;
+    }
+    fftn(F.data(), +1);
+    std::copy(F.begin(), F.end(), f);
 }
 static void dcomp_real(const double *f, int d, double *out)
 {
@@ -597,6 +614,23 @@ static void apply_hamiltonian(int it, std::vector<Complex> &w, Complex *out)
         dcomp_real(Ab[d], d, dA[1][d].data());
     }
 #endif
+#ifdef ENABLE_VELOCITY_EXT
+    /* kernel_get_vector_vext + compute_divergence_real_vector_f (pca_kernels.cu:623-640, 743-757) */
+    std::vector<double> vel[2][3], divv[2];
+    for (int sp = 0; sp < 2; sp++) {
+        divv[sp].assign(N, 0.0);
+        for (int d = 0; d < 3; d++) vel[sp][d].assign(N, 0.0);
+        for (int i = 0; i < N; i++) {
+            int ix, iy, iz; decode(i, ix, iy, iz);
+            for (int d = 0; d < CODEDIM; d++) vel[sp][d][i] = ORC_VEL_EXT(ix, iy, iz, it, sp == 0 ? SPINA : SPINB, d);
+        }
+        std::vector<double> t(N);
+        for (int d = 0; d < CODEDIM; d++) {
+            dcomp_real(vel[sp][d].data(), d, t.data());
+            for (int i = 0; i < N; i++) divv[sp][i] += t[i];
+        }
+    }
+#endif
     std::vector<Complex> Dt(N);
     for (int i = 0; i < N; i++) {
         int ix, iy, iz; decode(i, ix, iy, iz);
@@ -623,10 +657,29 @@ static void apply_hamiltonian(int it, std::vector<Complex> &w, Complex *out)
             double cja = 0.0, cjb = 0.0;
 #ifdef BDG_MODE
             double p = 0.5 * kp2;
+#ifdef ENABLE_VELOCITY_EXT
+            /* kernel_apply_hamiltonian_bdg with the velocity terms (pca_kernels.cu:432-480) */
+            Complex gav[3], gbv[3];
+            for (int d = 0; d < 3; d++) {
+                gav[d] = Complex(0.0, 1.0 * vel[0][d][i]);
+                gbv[d] = Complex(0.0, -1.0 * vel[1][d][i]);
+            }
+            cja = 0.5 * divv[0][i];
+            cjb = 0.5 * divv[1][i];
+#endif
             u += tu * Complex(Va - dc_mu_a + p, cja);
             v -= tv * Complex(Vb - dc_mu_b + p, -1.0 * cjb);
             u += tv * D;
             v += tu * std::conj(D);
+#ifdef ENABLE_VELOCITY_EXT
+            {
+                std::vector<Complex> *dd[3] = {&ddx, &ddy, &ddz};
+                for (int d = 0; d < CODEDIM; d++) {
+                    u += U(*dd[d], n)[i] * gav[d];
+                    v -= V(*dd[d], n)[i] * gbv[d];
+                }
+            }
+#endif
             u += lu * (-0.5);
             v -= lv * (-0.5);
 #else
@@ -647,6 +700,15 @@ static void apply_hamiltonian(int it, std::vector<Complex> &w, Complex *out)
                 ga[d] += Complex(0.0, -1. * Aa[d][i]);
                 gb[d] += Complex(0.0, 1. * Ab[d][i]);
             }
+#ifdef ENABLE_VELOCITY_EXT
+            /* pca_kernels.cu:315-327 */
+            for (int d = 0; d < CODEDIM; d++) {
+                ga[d] += Complex(0.0, 1.0 * vel[0][d][i]);
+                gb[d] += Complex(0.0, -1.0 * vel[1][d][i]);
+            }
+            cja += 0.5 * divv[0][i];
+            cjb += 0.5 * divv[1][i];
+#endif
 #endif
             u += tu * Complex(Va - dc_mu_a + ja, cja);
             v -= tv * Complex(Vb - dc_mu_b + jb, -1.0 * cjb);
@@ -708,6 +770,19 @@ static void half_step_densities(int it_next, int grads)
         high_k_filter(P.alpha_b);
     }
 #endif
+    /* the fields apply_hamiltonian filters in place before building H: V_a, V_b
+     * (pca_kernels.cu:700-704), delta (mode 2, :758-762), the A components with current
+     * corrections outside BdG (:791-795) */
+    if (hkf_mode >= 1) {
+        wslda_potential P = pots_view(pots.data());
+        high_k_filter(P.V_a);
+        high_k_filter(P.V_b);
+        if (hkf_mode >= 2) high_k_filter_c(P.delta);
+#if defined(CURRENT_CORRECTIONS) && !defined(BDG_MODE)
+        double *A[6] = {P.A_a_x, P.A_a_y, P.A_a_z, P.A_b_x, P.A_b_y, P.A_b_z};
+        for (int k = 0; k < 6; k++) high_k_filter(A[k]);
+#endif
+    }
     alpha_laplace(y);
 }
 
@@ -868,6 +943,16 @@ int orc_energy(double *E)
 #endif
 #ifdef ENABLE_DELTA_EXT
         e[EPAIREXT * (size_t)N + i] = (std::conj(Dn.nu[i]) * ORC_D_EXT(ix, iy, iz, it, P.delta[i])).real() * (-2.0) * VOL;
+#endif
+#ifdef ENABLE_VELOCITY_EXT
+        /* kernel_compute_energy_velocity_ext (pca_kernels.cu:163-187; 2D/1D over their axes) */
+        {
+            const double *ja[3] = {Dn.j_a_x, Dn.j_a_y, Dn.j_a_z}, *jb[3] = {Dn.j_b_x, Dn.j_b_y, Dn.j_b_z};
+            double sv = 0.0;
+            for (int d = 0; d < CODEDIM; d++)
+                sv += ja[d][i] * ORC_VEL_EXT(ix, iy, iz, it, SPINA, d) + jb[d][i] * ORC_VEL_EXT(ix, iy, iz, it, SPINB, d);
+            e[EVELEXT * (size_t)N + i] = sv * (-1.0) * VOL;
+        }
 #endif
         e[NPARTA * (size_t)N + i] = na;
         e[NPARTB * (size_t)N + i] = nb;

@@ -33,6 +33,9 @@ CASES = {
     "c3_aslda3d": (8, 2, 1, False),
     "c4_bdg2d": (16, 4, 1, False),
     "c5_slda3d": (4, 2, 1, False),
+    "t2d_vext": (24, 3, 2, True),
+    "t1d_bdg_vext": (24, 3, 2, True),
+    "t2d_big": (8, 3, 1, False),
 }
 
 # effective-mass filter cases (pca.c:1448-1453, hkf_mode 1): the same runs with alpha_a,
@@ -44,11 +47,22 @@ HKF_CASES = {
     "c3_aslda3d": (8, 2, 1, False),
 }
 HKF_FRACTIONS = (0.35, 0.04)
+# hkf_mode 2 also filters the pairing field (apply_hamiltonian, pca_kernels.cu:758-762)
+HKF2_CASES = {
+    "t2d_slda": (24, 3, 2, True),
+    "t3d_aslda": (24, 3, 2, True),
+}
 
 
-def hkf_params(proj):
+def hkf_params(proj, mode=1):
     emax = 0.5 * np.pi ** 2 / proj.dx ** 2
-    return 1, HKF_FRACTIONS[0] * emax, HKF_FRACTIONS[1] * emax
+    return mode, HKF_FRACTIONS[0] * emax, HKF_FRACTIONS[1] * emax
+
+
+
+
+def fixture_suffix(hkf):
+    return {0: "", 1: "_hkf", 2: "_hkf2"}[hkf]
 
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -99,13 +113,13 @@ def slim(rec, n):
     return rec
 
 
-def run_case(name, out_dir, hkf=False):
-    nwf, nsteps, nmeas, full = (HKF_CASES if hkf else CASES)[name]
+def run_case(name, out_dir, hkf=0):
+    nwf, nsteps, nmeas, full = {0: CASES, 1: HKF_CASES, 2: HKF2_CASES}[hkf][name]
     proj, y0, occ, pots, params, extra = case_inputs(name, nwf)
     so = os.path.join(REPO, "oracle", "_ref", name, "libref.so")
     lib = ctypes.CDLL(so, mode=ctypes.RTLD_LOCAL)
     lib.refh_set_hkf.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
-    mode, mu, T = hkf_params(proj) if hkf else (0, 0.0, 1.0)
+    mode, mu, T = hkf_params(proj, hkf) if hkf else (0, 0.0, 1.0)
     lib.refh_set_hkf(mode, mu, T)
     lib.refh_numel.restype = ctypes.c_int
     lib.refh_nhist.restype = ctypes.c_int
@@ -139,7 +153,7 @@ def run_case(name, out_dir, hkf=False):
     if hkf:
         rec["hkf"] = np.array([mode, mu, T])
     rec = slim(rec, n)
-    path = os.path.join(out_dir, f"{name}_hkf.npz" if hkf else f"{name}.npz")
+    path = os.path.join(out_dir, f"{name}{fixture_suffix(hkf)}.npz")
     np.savez_compressed(path, **rec)
     print(f"{name}: nwf={nwf} steps={nsteps}x{nmeas} E={en[:7].sum():.12g} N={en[7]:.12g},{en[8]:.12g} "
           f"ms/step={ms[0]:.3f} -> {path}")
@@ -149,7 +163,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--slim-existing", action="store_true", help="apply slim() to fixtures in --out")
-    ap.add_argument("--hkf", action="store_true", help="the effective-mass filter cases (HKF_CASES)")
+    ap.add_argument("--hkf", type=int, default=0, choices=[0, 1, 2],
+                    help="1: the effective-mass filter cases (HKF_CASES); 2: masses and pairing field (HKF2_CASES)")
     ap.add_argument("projects", nargs="*")
     a = ap.parse_args()
     if a.slim_existing:
@@ -162,7 +177,7 @@ def main():
                     np.savez_compressed(path, **slim(rec, n))
         return
     os.makedirs(a.out, exist_ok=True)
-    for name in (a.projects or list(HKF_CASES if a.hkf else CASES)):
+    for name in (a.projects or list({0: CASES, 1: HKF_CASES, 2: HKF2_CASES}[a.hkf])):
         run_case(name, a.out, hkf=a.hkf)
 
 

@@ -11,7 +11,7 @@ import pytest
 from parity_util import density_errors, rel, run_gpu, run_oracle
 
 TOL = 1e-10
-SMALL = ["t1d_custom", "t1d_aslda", "t2d_slda", "t2d_bdg", "t3d_slda", "t3d_aslda"]
+SMALL = ["t1d_custom", "t1d_aslda", "t2d_slda", "t2d_bdg", "t3d_slda", "t3d_aslda", "t2d_vext", "t1d_bdg_vext"]
 
 
 def _compare(name, nwf, nsteps, nmeas, tol=TOL, hkf=None):
@@ -41,7 +41,7 @@ def test_small_projects_fp64(has_gpu, name):
 
 @pytest.mark.gpu
 def test_c1_bdg1d_full_config(has_gpu):
-    """1D TD-BdG, NX=128, 256 states, 100 steps: densities after 100 steps."""
+    """the 1D TD-BdG workload, NX=128, 256 states, 100 steps: densities after 100 steps."""
     _compare("c1_bdg1d", nwf=256, nsteps=100, nmeas=1)
 
 
@@ -68,12 +68,22 @@ def test_c5_slda3d_small_s(has_gpu):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name,nwf,nsteps", [("t1d_aslda", 24, 3), ("t3d_aslda", 24, 3), ("c3_aslda3d", 8, 2)])
-def test_high_k_filter_of_masses(has_gpu, name, nwf, nsteps):
-    """variable-mass runs with the effective-mass filter (pca.c:1448-1453) on: fused path
-    (t1d, t3d) and staged plane/pencil path (c3, 32^3)"""
+@pytest.mark.parametrize("name,nwf,nsteps,mode", [("t1d_aslda", 24, 3, 1), ("t3d_aslda", 24, 3, 1), ("c3_aslda3d", 8, 2, 1),
+                                                  ("t2d_slda", 24, 3, 2), ("t3d_aslda", 24, 3, 2), ("c3_aslda3d", 8, 2, 2),
+                                                  ("t2d_vext", 24, 3, 2)])
+def test_high_k_filters(has_gpu, name, nwf, nsteps, mode):
+    """runs with the high-k filters on: mode 1 filters the effective masses after every
+    functional evaluation (pca.c:1448-1453), mode 2 the pairing field too; fused path (t1d,
+    t2d, t3d) and staged plane/pencil path (c3, 32^3)"""
     import sys, os
     sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
     from golden.make_golden import hkf_params
     from wslda_b200.projects import Project
-    _compare(name, nwf=nwf, nsteps=nsteps, nmeas=2 if nsteps == 3 else 1, hkf=hkf_params(Project(name)))
+    _compare(name, nwf=nwf, nsteps=nsteps, nmeas=2 if nsteps == 3 else 1, hkf=hkf_params(Project(name), mode))
+
+
+@pytest.mark.gpu
+def test_t2d_big_staged(has_gpu):
+    """2D 160x96 ASLDA: a radix-5 axis longer than 128 points and a state too large for one
+    CTA, so the 2D plane/pencil path"""
+    _compare("t2d_big", nwf=8, nsteps=3, nmeas=1)

@@ -8,7 +8,7 @@ import pytest
 
 from parity_util import density_errors, inputs, rel, run_oracle
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
-from golden.make_golden import CASES, HKF_CASES, state_moments  # noqa: E402
+from golden.make_golden import CASES, HKF2_CASES, HKF_CASES, state_moments  # noqa: E402
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 TOL = 1e-10
@@ -17,14 +17,15 @@ TOL = 1e-10
 def _cases():
     plain = [n for n in CASES if os.path.exists(os.path.join(GOLDEN, f"{n}.npz"))]
     hkf = [f"{n}_hkf" for n in HKF_CASES if os.path.exists(os.path.join(GOLDEN, f"{n}_hkf.npz"))]
-    return plain + hkf
+    hkf2 = [f"{n}_hkf2" for n in HKF2_CASES if os.path.exists(os.path.join(GOLDEN, f"{n}_hkf2.npz"))]
+    return plain + hkf + hkf2
 
 
 @pytest.mark.parametrize("name", _cases())
 def test_oracle_matches_reference_golden(name):
     g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
     hkf = tuple(g["hkf"]) if "hkf" in g.files else None
-    name = name[:-4] if name.endswith("_hkf") else name
+    name = name.rsplit("_hkf", 1)[0]
     nwf, nsteps, nmeas = int(g["nwf"]), int(g["nsteps"]), int(g["nmeas"])
     proj, d = inputs(name, nwf)
     # the regenerated inputs are the ones the fixture was made from

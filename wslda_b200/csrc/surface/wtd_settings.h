@@ -52,7 +52,7 @@
 #endif
 
 #if FUNCTIONAL==SLDAE
-#error "FUNCTIONAL SLDAE is not provided by this library (see DESIGN.md, scope)"
+#error "FUNCTIONAL SLDAE is not provided by this library"
 #endif
 
 /* mode derivation (pca_settings.h:75-95, 186-222) */
@@ -108,11 +108,14 @@
 #define FAST_CONST_EFFECTIVE_MASS_MODE
 #endif
 #endif
+/* an external velocity field needs the gradient (current) terms of H: variable-mass path
+ * (pca_settings.h:217-220) */
 #ifdef ENABLE_VELOCITY_EXT
-#error "ENABLE_VELOCITY_EXT is not provided by this library (see DESIGN.md, scope)"
+#define CURRENT_CORRECTIONS
+#undef FAST_CONST_EFFECTIVE_MASS_MODE
 #endif
 #ifdef SPINSYMMETRY_MODE
-#error "SPINSYMMETRY_MODE is not provided by this library (see DESIGN.md, scope)"
+#error "SPINSYMMETRY_MODE is not provided by this library"
 #endif
 
 #if REGULARIZATION_SCHEME==CUBIC_CUTOFF

@@ -78,7 +78,7 @@ __device__ __forceinline__ void nu_adjoint(double2 &gu, double2 &gv, double2 nb,
 
 /* laplacian of the two fields in (BU, BV), in place */
 template <class G>
-__device__ __forceinline__ void lap2(double2 *BU, double2 *BV, const double2 *tw, const double (*kt)[128])
+__device__ __forceinline__ void lap2(double2 *BU, double2 *BV, const double2 *tw, const double (*kt)[WTD_KT])
 {
     __syncthreads();
     fft_forward<G, 2>(BU, (int)(BV - BU), tw);
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(512, 1) k_adj_B(AdjArgs a, const double2 *gtw,
     double2 *BU = (double2 *)smem_raw;
     double2 *BV = BU + G::padded;
     double2 *tw = BV + G::padded;
-    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + G::twtotal);
     double *red = (double *)(kt + 6);
     load_tables<G>(tw, kt, gtw, gk);
     double *ds = a.slots + (size_t)blockIdx.x * 4 * N;
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(512, 1) k_adj_A(AdjArgs a, const double2 *gtw,
     double2 *BU = (double2 *)smem_raw;
     double2 *BV = BU + G::padded;
     double2 *tw = BV + G::padded;
-    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + G::twtotal);
     double *red = (double *)(kt + 6);
     load_tables<G>(tw, kt, gtw, gk);
     double *ds = a.slots + (size_t)blockIdx.x * 4 * N;

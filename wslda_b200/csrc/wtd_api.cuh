@@ -195,20 +195,46 @@ static int ensure_fk(wtd_ctx *c)
     return WTD_OK;
 }
 
-/* high-k filter of alpha_a and alpha_b after the functional (hkf_mode >= 1), as the
- * reference's driver does for variable-mass runs (pca.c:1448-1453, cpca.c:1014-1017) */
-static int filter_masses(wtd_ctx *c)
+/* high-k filters of the fields H is built from, once after every functional evaluation, as
+ * the reference does (in place) between compute_potentials and the H application:
+ *   hkf_mode >= 1: alpha_a, alpha_b in variable-mass runs (driver, pca.c:1448-1453), V_a, V_b
+ *                  (apply_hamiltonian, pca_kernels.cu:700-704) and, with current corrections
+ *                  outside BdG, the six A components (pca_kernels.cu:791-795);
+ *   hkf_mode >= 2: also the pairing field (pca_kernels.cu:758-762) */
+static int filter_fields(wtd_ctx *c)
 {
     if (c->hkf_mode < 1) return WTD_OK;
     constexpr size_t N = WTD_NUMEL;
-    double *alpha = c->pots + 4 * N; /* alpha_a, alpha_b consecutive */
-    if (WTD_BIG) return big_filter_real(alpha, 2, c->hkf_mu, c->hkf_T, c->stage3d, c->tw, c->ktab, c->st);
     constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
+    struct { double *f; int nf; } real[3] = {{c->pots, 2}, {NULL, 0}, {NULL, 0}};   /* V_a, V_b */
+    if (WTD_VAR) real[1] = {c->pots + 4 * N, 2};                                    /* alpha_a, alpha_b */
+#if defined(CURRENT_CORRECTIONS) && !defined(BDG_MODE)
+    real[2] = {c->pots + 6 * N, 6};                                                 /* A_a xyz, A_b xyz */
+#endif
+    double2 *delta = (double2 *)(c->pots + 2 * N);
+    if (WTD_BIG) {
+        for (int k = 0; k < 3; k++)
+            if (real[k].f) WTD_TRY(big_filter_real(real[k].f, real[k].nf, c->hkf_mu, c->hkf_T, c->stage3d, c->tw, c->ktab, c->st));
+        if (c->hkf_mode >= 2)
+            WTD_TRY(big_derivs(delta, 1, delta, NULL, NULL, NULL, c->tw, c->ktab, c->st, 1, c->hkf_mu, c->hkf_T));
+        return WTD_OK;
+    }
     if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     static bool attr = false;
-    if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_hkf_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
-    wtd_hkf_kernel<WG><<<2, 512, sm, c->st>>>(alpha, c->hkf_mu, c->hkf_T, c->tw, c->ktab);
-    WTD_LAUNCHED(c);
+    if (!attr) {
+        WTD_CU(cudaFuncSetAttribute(wtd_hkf_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        WTD_CU(cudaFuncSetAttribute(wtd_hkf_c_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        attr = true;
+    }
+    for (int k = 0; k < 3; k++)
+        if (real[k].f) {
+            wtd_hkf_kernel<WG><<<real[k].nf, 512, sm, c->st>>>(real[k].f, c->hkf_mu, c->hkf_T, c->tw, c->ktab);
+            WTD_LAUNCHED(c);
+        }
+    if (c->hkf_mode >= 2) {
+        wtd_hkf_c_kernel<WG><<<1, 512, sm, c->st>>>(delta, delta, c->hkf_mu, c->hkf_T, c->tw, c->ktab);
+        WTD_LAUNCHED(c);
+    }
     return WTD_OK;
 }
 
@@ -238,9 +264,7 @@ static int after_pass(wtd_ctx *c, bool full, int it)
     modify_potentials<<<pb, 128, 0, c->st>>>(it, D, P);
     WTD_LAUNCHED(c);
 #endif
-#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
-    WTD_TRY(filter_masses(c));
-#endif
+    WTD_TRY(filter_fields(c));
     wtd_prep_coef<<<pb, 128, 0, c->st>>>(it, P, c->cf);
     WTD_LAUNCHED(c);
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
@@ -281,7 +305,7 @@ static int staged_densities(wtd_ctx *c, bool grads)
 static int staged_derivs(wtd_ctx *c, bool grads)
 {
     const int nf = 2 * c->S;
-    if (grads) return big_derivs((double2 *)c->y, nf, c->dlap, c->ddx, c->ddy, c->ddz, c->tw, c->ktab, c->st);
+    if (grads) return big_derivs((double2 *)c->y, nf, c->dlap, c->ddx, c->ddy, CODEDIM >= 3 ? c->ddz : NULL, c->tw, c->ktab, c->st);
     return big_derivs((double2 *)c->y, nf, c->dlap, NULL, NULL, NULL, c->tw, c->ktab, c->st);
 }
 
@@ -297,9 +321,7 @@ static int staged_potentials(wtd_ctx *c, int it)
     modify_potentials<<<pb, 128, 0, c->st>>>(it, D, P);
     WTD_LAUNCHED(c);
 #endif
-#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
-    WTD_TRY(filter_masses(c));
-#endif
+    WTD_TRY(filter_fields(c));
     wtd_prep_coef<<<pb, 128, 0, c->st>>>(it, P, c->cf);
     WTD_LAUNCHED(c);
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
@@ -474,7 +496,7 @@ size_t wtd_device_bytes(int nwf, int precision)
     size_t n2 = (size_t)2 * nwf * WTD_NUMEL;
     size_t b = n2 * (elem_bytes_y(precision) + WTD_NHIST * elem_bytes_h(precision)) +
                (size_t)300 * 12 * WTD_NUMEL * sizeof(double);
-    if (WTD_BIG) b += n2 * sizeof(double2) * (WTD_VAR ? 5 : 4);
+    if (WTD_BIG) b += n2 * sizeof(double2) * ((CODEDIM >= 3 ? 4 : 3) + (WTD_VAR ? 1 : 0));
     return b;
 }
 
@@ -540,12 +562,12 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     ALLOC(c->ework, (size_t)TDWSLDAITEMS * N * sizeof(double));
     ALLOC(c->eout, 16 * sizeof(double));
     ALLOC(c->tw, WG::twtotal * sizeof(double2));
-    ALLOC(c->ktab, 6 * 128 * sizeof(double));
+    ALLOC(c->ktab, 6 * WTD_KT * sizeof(double));
     if (precision != WTD_FP64) ALLOC(c->stage, n2 * sizeof(double2));
     if (c->staged) {
         ALLOC(c->ddx, n2 * sizeof(double2));
         ALLOC(c->ddy, n2 * sizeof(double2));
-        ALLOC(c->ddz, n2 * sizeof(double2));
+        if (CODEDIM >= 3) ALLOC(c->ddz, n2 * sizeof(double2));
         ALLOC(c->dlap, n2 * sizeof(double2));
         if (WTD_VAR) ALLOC(c->dalap, n2 * sizeof(double2));
         ALLOC(c->stage3d, 2 * N * sizeof(double2));
@@ -558,7 +580,7 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     cudaMemsetAsync(c->dens, 0, 12 * N * sizeof(double), c->st);
     {
         double2 tw[WG::twtotal];
-        double kt[6 * 128];
+        double kt[6 * WTD_KT];
         wtd_make_tables(tw, kt);
         cudaMemcpyAsync(c->tw, tw, sizeof(tw), cudaMemcpyHostToDevice, c->st);
         cudaMemcpyAsync(c->ktab, kt, sizeof(kt), cudaMemcpyHostToDevice, c->st);

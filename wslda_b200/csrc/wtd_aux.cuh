@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(512) wtd_tau_kernel(double *dens, const double
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *B = (double2 *)smem_raw;
     double2 *tw = B + G::padded;
-    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + G::twtotal);
     load_tables<G>(tw, kt, gtw, gk);
     constexpr int N = G::ntot;
     double *rho = dens + (blockIdx.x == 0 ? 2 : 7) * (size_t)N;
@@ -74,23 +74,40 @@ __global__ void wtd_prep_coef(int it, wslda_potential P, double *cf)
     cf[CF_VB * N + i] = P.V_b[i] - dc_mu_b;
     cf[CF_DRE * N + i] = D.real();
     cf[CF_DIM * N + i] = D.imag();
-#if defined(BDG_MODE)
+#if defined(BDG_MODE) && defined(FAST_CONST_EFFECTIVE_MASS_MODE)
     cf[CF_AA * N + i] = -0.5;
     cf[CF_AB * N + i] = -0.5;
 #elif defined(FAST_CONST_EFFECTIVE_MASS_MODE)
     cf[CF_AA * N + i] = P.alpha_a[i] * -0.5;
     cf[CF_AB * N + i] = P.alpha_b[i] * -0.5;
 #else
-    cf[CF_AA * N + i] = P.alpha_a[i] * -0.25;
-    cf[CF_AB * N + i] = P.alpha_b[i] * -0.25;
-    cf[CF_ALA * N + i] = P.alpha_a[i];
-    cf[CF_ALB * N + i] = P.alpha_b[i];
-    cf[CF_AAX * N + i] = P.A_a_x[i];
-    cf[CF_ABX * N + i] = P.A_b_x[i];
-    cf[CF_AAY * N + i] = (CODEDIM >= 2) ? P.A_a_y[i] : 0.0;
-    cf[CF_ABY * N + i] = (CODEDIM >= 2) ? P.A_b_y[i] : 0.0;
-    cf[CF_AAZ * N + i] = (CODEDIM >= 3) ? P.A_a_z[i] : 0.0;
-    cf[CF_ABZ * N + i] = (CODEDIM >= 3) ? P.A_b_z[i] : 0.0;
+#ifdef BDG_MODE
+    /* BdG with a velocity field: -1/2 lap, gradient terms only (pca_kernels.cu:393-495) */
+    const double ala = 1.0, alb = 1.0;
+    double Aa[3] = {0.0, 0.0, 0.0}, Ab[3] = {0.0, 0.0, 0.0};
+#else
+    const double ala = P.alpha_a[i], alb = P.alpha_b[i];
+    double Aa[3] = {P.A_a_x[i], (CODEDIM >= 2) ? P.A_a_y[i] : 0.0, (CODEDIM >= 3) ? P.A_a_z[i] : 0.0};
+    double Ab[3] = {P.A_b_x[i], (CODEDIM >= 2) ? P.A_b_y[i] : 0.0, (CODEDIM >= 3) ? P.A_b_z[i] : 0.0};
+#endif
+#ifdef ENABLE_VELOCITY_EXT
+    /* the external velocity enters as A - v: gradient coefficient i v and +div(v)/2
+     * (pca_kernels.cu:315-327, the divergence taken spectrally like div A) */
+    for (int d = 0; d < CODEDIM; d++) {
+        Aa[d] -= WTD_VEL_EXT(ix, iy, iz, it, SPINA, d);
+        Ab[d] -= WTD_VEL_EXT(ix, iy, iz, it, SPINB, d);
+    }
+#endif
+    cf[CF_AA * N + i] = ala * -0.25;
+    cf[CF_AB * N + i] = alb * -0.25;
+    cf[CF_ALA * N + i] = ala;
+    cf[CF_ALB * N + i] = alb;
+    cf[CF_AAX * N + i] = Aa[0];
+    cf[CF_ABX * N + i] = Ab[0];
+    cf[CF_AAY * N + i] = Aa[1];
+    cf[CF_ABY * N + i] = Ab[1];
+    cf[CF_AAZ * N + i] = Aa[2];
+    cf[CF_ABZ * N + i] = Ab[2];
 #endif
 }
 
@@ -102,7 +119,7 @@ __global__ void __launch_bounds__(256) wtd_prep_var(double *cf, const double2 *g
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *B = (double2 *)smem_raw;
     double2 *tw = B + G::padded;
-    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + G::twtotal);
     load_tables<G>(tw, kt, gtw, gk);
     constexpr int N = G::ntot;
     const int s = blockIdx.x;
@@ -143,7 +160,7 @@ __global__ void __launch_bounds__(512) wtd_hkf_kernel(double *f, double mu, doub
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *B = (double2 *)smem_raw;
     double2 *tw = B + G::padded;
-    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + G::twtotal);
     load_tables<G>(tw, kt, gtw, gk);
     constexpr int N = G::ntot;
     double *a = f + (size_t)blockIdx.x * N;
@@ -175,7 +192,7 @@ __global__ void __launch_bounds__(512) wtd_hkf_c_kernel(const double2 *in, doubl
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *B = (double2 *)smem_raw;
     double2 *tw = B + G::padded;
-    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + G::twtotal);
     load_tables<G>(tw, kt, gtw, gk);
     constexpr int N = G::ntot;
     for (int p = threadIdx.x; p < N; p += blockDim.x) B[G::off(p)] = in[p];

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(512) k_derivs(const double2 *in, double2 *odx,
     double2 *B0 = (double2 *)smem_raw;
     double2 *W = B0 + G::padded;
     double2 *tw = W + G::padded;
-    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + G::twtotal);
     load_tables<G>(tw, kt, gtw, gk);
     constexpr int N = G::ntot;
     const size_t base = (size_t)blockIdx.x * N;
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(512) k_real_deriv(const double *f, double *out
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *B = (double2 *)smem_raw;
     double2 *tw = B + G::padded;
-    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + G::twtotal);
     load_tables<G>(tw, kt, gtw, gk);
     constexpr int N = G::ntot;
     for (int p = threadIdx.x; p < N; p += blockDim.x) B[G::off(p)] = make_double2(f[p], 0.0);
@@ -324,7 +324,7 @@ static int compat_tables(void)
 {
     if (g_tw) return 0;
     double2 tw[WG::twtotal];
-    double kt[6 * 128];
+    double kt[6 * WTD_KT];
     wtd_make_tables(tw, kt);
     if (cudaMalloc((void **)&g_tw, sizeof(tw)) != cudaSuccess) return WTD_ERR_NOMEM;
     if (cudaMalloc((void **)&g_ktab, sizeof(kt)) != cudaSuccess) return WTD_ERR_NOMEM;
@@ -626,7 +626,8 @@ int compute_derivatives(int n, wtd_z *wf, wtd_z *dx, wtd_z *dy, wtd_z *dz, wtd_z
     int r = compat_tables();
     if (r) return r;
     if (WTD_BIG) {
-        WTD_TRY(big_derivs((double2 *)wf, n, (double2 *)lap, (double2 *)dx, (double2 *)dy, (double2 *)dz, g_tw, g_ktab, 0));
+        WTD_TRY(big_derivs((double2 *)wf, n, (double2 *)lap, (double2 *)dx, (double2 *)dy,
+                           CODEDIM >= 3 ? (double2 *)dz : NULL, g_tw, g_ktab, 0));
         return cu_sync_status();
     }
     if (k_derivs_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
@@ -807,6 +808,25 @@ static int apply_hamiltonian_impl(int it, int n, wtd_z *in, wtd_z *out, wtd_z *d
 {
     if (qfswitch > 0.0) return WTD_ERR_UNSUPPORTED;
     if (!g_work || g_nwfip < n) return WTD_ERR_STATE;
+    /* high-k filters of the fields, in place, as the reference's apply_hamiltonian: V_a, V_b
+     * (hkf_mode >= 1, pca_kernels.cu:700-704), delta (>= 2, :758-762), the A components
+     * (>= 1 with current corrections outside BdG, :791-795) */
+    if (md.hkf_mode >= 1) {
+        int rf = high_frequency_filter_massive_d(2, pots, pots, md.hkf_mu, md.hkf_T, 512);
+        if (rf) return rf;
+    }
+    if (md.hkf_mode >= 2) {
+        wtd_z *delta = (wtd_z *)(pots + 2 * (size_t)WTD_NUMEL);
+        int rf = high_frequency_filter_c(delta, delta, md.hkf_mu, md.hkf_T, 512);
+        if (rf) return rf;
+    }
+#if defined(CURRENT_CORRECTIONS) && !defined(BDG_MODE)
+    if (md.hkf_mode >= 1) {
+        double *A = pots + 6 * (size_t)WTD_NUMEL;
+        int rf = high_frequency_filter_massive_d(6, A, A, md.hkf_mu, md.hkf_T, 512);
+        if (rf) return rf;
+    }
+#endif
     int r = compat_coefficients(it, pots);
     if (r) return r;
     r = compat_planewave(n, kky, kkz, NULL);

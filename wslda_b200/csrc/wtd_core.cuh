@@ -13,8 +13,10 @@
  * e^{+2 pi i k n/N}, unnormalised; the 1/N of the reference's derivative kernels
  * (hpc-engine/pca_derivative.cu:163-166) is folded into the k-space multiplier.
  *
- * Radices 8, 4, 2 and 3 cover every lattice size the reference accepts up to 128 points per
- * axis whose prime factors are 2 and 3 (NX, NY, NZ even, wslda_predefines_test.h:10-36).
+ * Radices 8, 4, 2 and 3 have hand-written butterflies; any other prime factor p of an axis
+ * (5, 7, 11, ... — the reference accepts every even extent, wslda_predefines_test.h:10-36)
+ * takes a direct p-point DFT whose roots of unity are read from the axis twiddle table
+ * (w_p^m = w_n^{m n/p}), so every even lattice size transforms exactly as with cuFFT.
  */
 #ifndef WTD_CORE_CUH
 #define WTD_CORE_CUH
@@ -63,7 +65,8 @@ template <> __device__ __forceinline__ float2 from_d<float2>(double2 a) { return
  * -------------------------------------------------------------------------------------*/
 __host__ __device__ constexpr int pad_index(int fast_index) { return fast_index + (fast_index >> 3); }
 
-__host__ __device__ constexpr int radix_first(int n) { return (n % 8 == 0) ? 8 : (n % 4 == 0) ? 4 : (n % 2 == 0) ? 2 : 3; }
+__host__ __device__ constexpr int smallest_odd_factor(int n, int p = 3) { return (p * p > n) ? n : (n % p == 0 ? p : smallest_odd_factor(n, p + 2)); }
+__host__ __device__ constexpr int radix_first(int n) { return (n % 8 == 0) ? 8 : (n % 4 == 0) ? 4 : (n % 2 == 0) ? 2 : smallest_odd_factor(n); }
 __host__ __device__ constexpr int radix_at(int n, int s) { return s == 0 ? radix_first(n) : radix_at(n / radix_first(n), s - 1); }
 __host__ __device__ constexpr int n_stages(int n) { return n <= 1 ? 0 : 1 + n_stages(n / radix_first(n)); }
 /* wave-number index of the digit-reversed output position p of an n-point DIF transform */
@@ -146,12 +149,31 @@ template <int SIGN, typename C> __device__ __forceinline__ void dft8(C *a)
     a[0] = e[0]; a[2] = e[1]; a[4] = e[2]; a[6] = e[3];
     a[1] = o[0]; a[3] = o[1]; a[5] = o[2]; a[7] = o[3];
 }
-template <int SIGN, int R, typename C> __device__ __forceinline__ void dft_r(C *a)
+/* direct R-point DFT for any other (prime) radix: X_k = sum_q x_q w_R^{SIGN' qk}, the roots
+ * taken from the axis table tw[t] = e^{-2 pi i t/n} at t = (qk mod R) * (n/R) */
+template <int SIGN, int R, typename C> __device__ __forceinline__ void dft_gen(C *a, const C *tw, int nR)
+{
+    C out[R];
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+        C acc = a[0];
+#pragma unroll
+        for (int q = 1; q < R; q++) {
+            const C w = tw[((q * k) % R) * nR];
+            acc = cadd(acc, SIGN < 0 ? cmul(a[q], w) : cmulc(a[q], w));
+        }
+        out[k] = acc;
+    }
+#pragma unroll
+    for (int k = 0; k < R; k++) a[k] = out[k];
+}
+template <int SIGN, int R, typename C> __device__ __forceinline__ void dft_r(C *a, const C *tw, int nR)
 {
     if constexpr (R == 8) dft8<SIGN>(a);
     else if constexpr (R == 4) dft4<SIGN>(a);
     else if constexpr (R == 2) dft2<SIGN>(a);
-    else dft3<SIGN>(a);
+    else if constexpr (R == 3) dft3<SIGN>(a);
+    else dft_gen<SIGN, R>(a, tw, nR);
 }
 
 /* ---------------------------------------------------------------------------------------
@@ -210,9 +232,9 @@ __device__ __forceinline__ void fft_stage(C *buf, int fstride, const C *tw)
             if (SIGN > 0) {
 #pragma unroll
                 for (int q = 1; q < R; q++) v[f][q] = cmulc(v[f][q], w[q]);
-                dft_r<SIGN, R>(v[f]);
+                dft_r<SIGN, R>(v[f], tw, n / R);
             } else {
-                dft_r<SIGN, R>(v[f]);
+                dft_r<SIGN, R>(v[f], tw, n / R);
 #pragma unroll
                 for (int q = 1; q < R; q++) v[f][q] = cmul(v[f][q], w[q]);
             }

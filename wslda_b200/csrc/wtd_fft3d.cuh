@@ -1,6 +1,7 @@
 /*
- * Spectral derivatives of 3D fields too large for one CTA's shared memory (32^3, 48^3 ...):
- * a plane/pencil decomposition through global memory.
+ * Spectral derivatives of fields too large for one CTA's shared memory (3D 32^3, 48^3 ...; 2D
+ * beyond about 74x74 in FP64): a plane/pencil decomposition through global memory.  In 2D a
+ * "plane" is one contiguous row along y.
  *
  *   k_planes  : one CTA per (field, x-plane) — 2D FFT over (y, z) of a contiguous plane in smem
  *   k_pencils : one CTA per (field, group of PX consecutive (y, z) pencils) — FFT along x,
@@ -18,7 +19,10 @@
 
 #include "wtd_step.cuh"
 
-#define WTD_PX 16   /* pencils per CTA */
+/* pencils per CTA: 16, or the largest power of two dividing NY*NZ (even, as every lattice
+ * extent the reference accepts) */
+#define WTD_NYZ ((NY) * (NZ))
+#define WTD_PX (WTD_NYZ % 16 == 0 ? 16 : WTD_NYZ % 8 == 0 ? 8 : WTD_NYZ % 4 == 0 ? 4 : 2)
 
 /* 2D (y, z) transform of plane x of field f: in -> out (may alias), fields of N points each */
 template <class GP, int SIGN>
@@ -27,7 +31,7 @@ __global__ void __launch_bounds__(512) k_planes(const double2 *in, double2 *out,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *B = (double2 *)smem_raw;
     double2 *tw = B + GP::padded;
-    double (*kt)[128] = (double (*)[128])(tw + GP::twtotal);
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + GP::twtotal);
     (void)kt;
     (void)nx;
     for (int t = threadIdx.x; t < GP::N0 + GP::N1; t += blockDim.x) tw[t] = gtw_yz[t];
@@ -52,10 +56,10 @@ __global__ void __launch_bounds__(512) k_pencils(const double2 *in, double2 *ola
     double2 *B0 = (double2 *)smem_raw;
     double2 *W = B0 + GX::padded;
     double2 *tw = W + GX::padded;
-    double (*kt)[128] = (double (*)[128])(tw + GX::twtotal);
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + GX::twtotal);
     constexpr int NXL = GX::N0, PX = GX::N1;
     for (int t = threadIdx.x; t < NXL; t += blockDim.x) tw[t] = gtw_x[t];
-    for (int t = threadIdx.x; t < 6 * 128; t += blockDim.x) kt[t / 128][t % 128] = gk[t];
+    for (int t = threadIdx.x; t < 6 * WTD_KT; t += blockDim.x) kt[t / WTD_KT][t % WTD_KT] = gk[t];
     const int groups = nyz / PX;
     const int f = blockIdx.x / groups, g = blockIdx.x - f * groups;
     const size_t fb = (size_t)f * N;

@@ -21,6 +21,11 @@
 #else
 #define WTD_U_EXT(ix, iy, iz, it, spin) 0.0
 #endif
+#if defined(ENABLE_VELOCITY_EXT)
+#define WTD_VEL_EXT(ix, iy, iz, it, spin, axis) velocity_ext(ix, iy, iz, it, spin, axis, dc_params, dc_extra_data_size, dc_extra_data)
+#else
+#define WTD_VEL_EXT(ix, iy, iz, it, spin, axis) 0.0
+#endif
 #if defined(ENABLE_DELTA_EXT)
 #define WTD_D_EXT(ix, iy, iz, it, d) delta_ext(ix, iy, iz, it, d, dc_params, dc_extra_data_size, dc_extra_data)
 #else
@@ -337,7 +342,18 @@ __global__ void wtd_energy_ext_kernel(int it, wslda_density Dn, wslda_potential 
 #else
     e[EPAIREXT * N + i] = 0.0;
 #endif
+#ifdef ENABLE_VELOCITY_EXT
+    /* -(j_a . v_a + j_b . v_b) (pca_kernels.cu:163-187; cpca/ccpca over their axes) */
+    {
+        const double *ja[3] = {Dn.j_a_x, Dn.j_a_y, Dn.j_a_z}, *jb[3] = {Dn.j_b_x, Dn.j_b_y, Dn.j_b_z};
+        double s = 0.0;
+        for (int d = 0; d < CODEDIM; d++)
+            s += ja[d][i] * WTD_VEL_EXT(ix, iy, iz, it, SPINA, d) + jb[d][i] * WTD_VEL_EXT(ix, iy, iz, it, SPINB, d);
+        e[EVELEXT * N + i] = s * (-1.0) * WTD_VOLEL;
+    }
+#else
     e[EVELEXT * N + i] = 0.0;
+#endif
     e[NPARTA * N + i] = na;
     e[NPARTB * N + i] = nb;
 #if CODEDIM >= 2

@@ -30,7 +30,7 @@ static constexpr size_t WTD_SMEM_MAX = 232448;
 static constexpr size_t k_field_smem = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
 static constexpr size_t k_derivs_smem = 2 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
 /* lattices whose fields exceed one CTA's shared memory take the plane/pencil transforms */
-static constexpr bool WTD_BIG = (CODEDIM == 3) && (k_derivs_smem > WTD_SMEM_MAX);
+static constexpr bool WTD_BIG = (CODEDIM >= 2) && (k_derivs_smem > WTD_SMEM_MAX);
 
 static inline int wtd_cuerr(cudaError_t e) { return e == cudaSuccess ? WTD_OK : WTD_ERR_CUDA; }
 #define WTD_TRY(x) do { int _r = (x); if (_r) return _r; } while (0)
@@ -40,7 +40,7 @@ static inline int wtd_cuerr(cudaError_t e) { return e == cudaSuccess ? WTD_OK : 
  * (rows 0-2 k_d, rows 3-5 k_d with the Nyquist mode zeroed) for this lattice */
 static void wtd_make_tables(double2 *tw, double *kt)
 {
-    memset(kt, 0, 6 * 128 * sizeof(double));
+    memset(kt, 0, 6 * WTD_KT * sizeof(double));
     const double Lax[3] = {LX, LY, LZ};
     for (int a = 0; a < 3; a++) {
         int n = WG::n(a);
@@ -48,11 +48,11 @@ static void wtd_make_tables(double2 *tw, double *kt)
             long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)t / (long double)n;
             tw[WG::twoff(a) + t] = make_double2((double)cosl(ang), -(double)sinl(ang));
         }
-        for (int p = 0; p < n && p < 128; p++) {
+        for (int p = 0; p < n && p < WTD_KT; p++) {
             int f = dif_freq(n, p);
             double k = (f < n / 2) ? 2. * M_PI / Lax[a] * (double)f : 2. * M_PI / Lax[a] * (double)(f - n);
-            kt[a * 128 + p] = (n > 1) ? k : 0.0;
-            kt[(3 + a) * 128 + p] = (n > 1 && f != n / 2) ? k : 0.0;
+            kt[a * WTD_KT + p] = (n > 1) ? k : 0.0;
+            kt[(3 + a) * WTD_KT + p] = (n > 1 && f != n / 2) ? k : 0.0;
         }
     }
 }

@@ -92,9 +92,13 @@ template <int NH> struct Abm {
 
 template <typename T> __device__ __forceinline__ double2 ld2(const T *p, size_t i) { return to_d(p[i]); }
 
+/* entries per axis of the wave-number tables: the longest lattice axis (at least 128) */
+#define WTD_KT_MAXN ((NX) > (NY) ? ((NX) > (NZ) ? (NX) : (NZ)) : ((NY) > (NZ) ? (NY) : (NZ)))
+#define WTD_KT (WTD_KT_MAXN > 128 ? ((WTD_KT_MAXN + 31) / 32) * 32 : 128)
+
 /* k-space multiplier tables: per axis, wave numbers of digit-reversed positions */
 template <class G> struct KTab {
-    double k[6][128];   /* rows 0-2: k_d of a digit-reversed position; rows 3-5: same with the
+    double k[6][WTD_KT];   /* rows 0-2: k_d of a digit-reversed position; rows 3-5: same with the
                            Nyquist mode set to 0 (first derivatives) */
 };
 
@@ -104,7 +108,7 @@ enum { OP_LAP = 0, OP_DX = 1, OP_DY = 2, OP_DZ = 3 };
 /* multiply a transformed field by the operator OP (1/N folded in): laplacian -|k|^2/N,
  * d/dx_d -> i k_d/N with the Nyquist mode zeroed (pca_derivative.cu:152-171) */
 template <class G, int OP, typename C>
-__device__ __forceinline__ void kmul(C *buf, const double (*kt)[128])
+__device__ __forceinline__ void kmul(C *buf, const double (*kt)[WTD_KT])
 {
     typedef decltype(buf[0].x) R;
     for (int i = threadIdx.x; i < G::ntot; i += blockDim.x) {
@@ -143,14 +147,14 @@ template <class G, typename TC, int NBUF> struct FusedSmem {
 
 /* load twiddles (e^{-2 pi i t/n} per axis) and the k tables into shared memory */
 template <class G, typename C>
-__device__ __forceinline__ void load_tables(C *tw, double (*kt)[128], const double2 *gtw, const double *gk)
+__device__ __forceinline__ void load_tables(C *tw, double (*kt)[WTD_KT], const double2 *gtw, const double *gk)
 {
     for (int t = threadIdx.x; t < G::twtotal; t += blockDim.x) {
         double2 w = gtw[t];
         C c; c.x = w.x; c.y = w.y;
         tw[t] = c;
     }
-    for (int t = threadIdx.x; t < 6 * 128; t += blockDim.x) kt[t / 128][t % 128] = gk[t];
+    for (int t = threadIdx.x; t < 6 * WTD_KT; t += blockDim.x) kt[t / WTD_KT][t % WTD_KT] = gk[t];
     __syncthreads();
 }
 
@@ -162,7 +166,7 @@ __device__ __forceinline__ void load_tables(C *tw, double (*kt)[128], const doub
 template <class G, typename TY, typename TC>
 __device__ __forceinline__ double hpsi_const(const TY *yu, const TY *yv, typename cplx<TC>::t *BU,
                                              typename cplx<TC>::t *BV, const typename cplx<TC>::t *tw,
-                                             const double (*kt)[128], const double *cf, double kp2, double *red)
+                                             const double (*kt)[WTD_KT], const double *cf, double kp2, double *red)
 {
     typedef typename cplx<TC>::t C;
     constexpr int N = G::ntot;
@@ -217,7 +221,7 @@ template <class G, typename TY, typename TC>
 __device__ __forceinline__ double hpsi_var(const TY *yu, const TY *yv, typename cplx<TC>::t *B0,
                                            typename cplx<TC>::t *W, typename cplx<TC>::t *HU,
                                            typename cplx<TC>::t *HV, const typename cplx<TC>::t *tw,
-                                           const double (*kt)[128], const double *cf, double kp2, double *red)
+                                           const double (*kt)[WTD_KT], const double *cf, double kp2, double *red)
 {
     typedef typename cplx<TC>::t C;
     constexpr int N = G::ntot;
@@ -332,7 +336,7 @@ __device__ __forceinline__ void dens_limited(double *ds, int p, int N, double2 u
 template <class G, typename TY, typename TC>
 __device__ __forceinline__ void dens_gradients(double *ds, const TY *ysrc, typename cplx<TC>::t *B0,
                                                typename cplx<TC>::t *W, const typename cplx<TC>::t *tw,
-                                               const double (*kt)[128], double f, double w, double kp2, int comp)
+                                               const double (*kt)[WTD_KT], double f, double w, double kp2, int comp)
 {
     typedef typename cplx<TC>::t C;
     constexpr int N = G::ntot;
@@ -387,7 +391,7 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
     C *B2 = BV + G::padded;
     C *B3 = B2 + G::padded;
     C *tw = BU + NBUF * G::padded;
-    double (*kt)[128] = (double (*)[128])(tw + G::twtotal);
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + G::twtotal);
     double *red = (double *)(kt + 6);
 
     load_tables<G>(tw, kt, gtw, gk);
