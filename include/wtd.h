@@ -87,6 +87,12 @@ int wtd_download_history(wtd_ctx *ctx, int slot, double *host);
 
 /* initial measurement (pca.c:939-958): normalise, all densities, tau; zero ABM history */
 int wtd_initial_measurement(wtd_ctx *ctx, int it0);
+/* Taylor self-start (pca.c:1086-1330, input "selfstart 1"), after wtd_initial_measurement:
+ * the first q steps (q = history length) are taken with a Taylor expansion of exp(-i H dt)
+ * (midpoint potentials from a half step), recording (H - <H>) psi of each start state as the
+ * ABM history; as in the reference, potentials and H use time index 0 during these steps and
+ * the time index does not advance.  FP64 only. */
+int wtd_selfstart(wtd_ctx *ctx);
 /* nsteps ABM steps forming one measurement block (pca.c:1401-1571): tau and j are formed on
  * the block's last step (constant mass) or on every step (variable mass) */
 int wtd_steps(wtd_ctx *ctx, int nsteps);

@@ -87,6 +87,15 @@ extern "C" int refh_nhist(void) { return nhist_of_scheme(); }
  * quasiparticle energies (nwf), history slots f1..fq in the reference's order after the last
  * pointer rotation (q x 2*nwf*N complex), and the device time per step in ms.
  */
+/* Taylor self-start of the history (pca.c:1086-1330), off unless set */
+static int selfstart_on = 0;
+extern "C" int taylor_expansion_contribution(int it, double dt, int n, Z *hpsi, Z *upd, Z *contr, int nthreads);
+extern "C" int refh_set_selfstart(int on)
+{
+    selfstart_on = on;
+    return 0;
+}
+
 /* effective-mass filtering of the reference driver (pca.c:1448-1453), off unless set */
 static int hkf_mode = 0;
 static double hkf_mu = 0.0, hkf_T = 1.0;
@@ -172,14 +181,24 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
 
     /* dimension-dependent call shapes */
 #if REF_CODEDIM == 3
-#define DENS(g) calculate_densities(nwf, d_wf, d_dx, d_dy, d_dz, d_lap, d_fb, NULL, d_dens, g, nthreads)
-#define HAPPLY(it, out) apply_hamiltonian(it, nwf, d_wf, out, d_dx, d_dy, d_dz, d_lap, d_alap, d_dens, d_pots, 0.0, NULL, 0.0, nthreads)
+#define DENSW(w, g) calculate_densities(nwf, w, d_dx, d_dy, d_dz, d_lap, d_fb, NULL, d_dens, g, nthreads)
+#define HAPPLYW(it, in, out, uq) apply_hamiltonian(it, nwf, in, out, d_dx, d_dy, d_dz, d_lap, d_alap, d_dens, d_pots, 0.0, uq, 0.0, nthreads)
 #elif REF_CODEDIM == 2
-#define DENS(g) calculate_densities(nwf, d_wf, d_dx, d_dy, d_lap, d_kk, d_fb, NULL, d_dens, g, nthreads)
-#define HAPPLY(it, out) apply_hamiltonian(it, nwf, d_wf, out, d_dx, d_dy, d_kk, d_lap, d_alap, d_dens, d_pots, 0.0, NULL, 0.0, nthreads)
+#define DENSW(w, g) calculate_densities(nwf, w, d_dx, d_dy, d_lap, d_kk, d_fb, NULL, d_dens, g, nthreads)
+#define HAPPLYW(it, in, out, uq) apply_hamiltonian(it, nwf, in, out, d_dx, d_dy, d_kk, d_lap, d_alap, d_dens, d_pots, 0.0, uq, 0.0, nthreads)
 #else
-#define DENS(g) calculate_densities(nwf, d_wf, d_dx, d_lap, d_kk, d_fb, NULL, d_cnt, d_dens, g, nthreads)
-#define HAPPLY(it, out) apply_hamiltonian(it, nwf, d_wf, out, d_dx, d_kk, d_lap, d_alap, d_dens, d_pots, 0.0, NULL, 0.0, nthreads)
+#define DENSW(w, g) calculate_densities(nwf, w, d_dx, d_lap, d_kk, d_fb, NULL, d_cnt, d_dens, g, nthreads)
+#define HAPPLYW(it, in, out, uq) apply_hamiltonian(it, nwf, in, out, d_dx, d_kk, d_lap, d_alap, d_dens, d_pots, 0.0, uq, 0.0, nthreads)
+#endif
+#define DENS(g) DENSW(d_wf, g)
+#define HAPPLY(it, out) HAPPLYW(it, d_wf, out, NULL)
+#define DERIVS(w, g) ((g) ? compute_derivatives(2 * nwf, w, d_dx, d_dy, d_dz, d_lap, nthreads) : compute_laplace(2 * nwf, w, d_lap, nthreads))
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+#define ALAP(w) do { CK(multiply_wf_by_alpha(nwf, w, d_alap, d_pots, nthreads)); CK(compute_laplace(2 * nwf, d_alap, d_alap, nthreads)); } while (0)
+#define HKF_ALPHA() do { if (hkf_mode >= 1) CK(high_frequency_filter_massive_d(2, d_pots + 4 * (size_t)RN, d_pots + 4 * (size_t)RN, hkf_mu, hkf_T, nthreads)); } while (0)
+#else
+#define ALAP(w) do { } while (0)
+#define HKF_ALPHA() do { } while (0)
 #endif
 
     int it = it0;
@@ -189,6 +208,66 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
     CK(compute_derivatives(2 * nwf, d_wf, d_dx, d_dy, d_dz, d_lap, nthreads));
     CK(DENS(grads));
     CK(density_caculate_tau(d_dens, nthreads));
+
+    if (selfstart_on) {
+        /* pca.c:1086-1330, restated over the reference's kernels */
+        const int q = nh, iters = (nh == 3) ? 4 : 5;
+#ifdef FAST_CONST_EFFECTIVE_MASS_MODE
+        const int sg = 0;
+#else
+        const int sg = 1;
+#endif
+        double *d_qpe = NULL;
+        CK(cudaMalloc((void **)&d_qpe, nwf * sizeof(double)));
+        Z *rec = alloc_z((size_t)q * M);
+        Z *f1 = d_f[0], *f2 = d_f[1], *f3 = d_f[2];
+        for (int step = 0; step < q; step++) {
+            CK(DERIVS(d_wf, sg));
+            CK(DENS(sg));
+            if (sg) CK(density_caculate_tau(d_dens, nthreads));
+            CK(compute_potentials(0, d_dens, d_pots, 1.0, nthreads));
+            HKF_ALPHA();
+            ALAP(d_wf);
+            CK(cudaMemcpy(f3, d_wf, M * sizeof(Z), cudaMemcpyDeviceToDevice));
+            CK(HAPPLYW(0, f3, f1, NULL));
+            CK(cudaMemcpy(d_qpe, d_work, nwf * sizeof(double), cudaMemcpyDeviceToDevice));
+            for (int h = q - 1; h > 0; h--) CK(cudaMemcpy(rec + (size_t)h * M, rec + (size_t)(h - 1) * M, M * sizeof(Z), cudaMemcpyDeviceToDevice));
+            CK(cudaMemcpy(rec, f1, M * sizeof(Z), cudaMemcpyDeviceToDevice));
+            CK(taylor_expansion_contribution(1, 0.5 * dt, nwf, f1, f3, f2, nthreads));
+            for (int m = 1; m < iters; m++) {
+                CK(DERIVS(f2, sg));
+                ALAP(f2);
+                CK(HAPPLYW(0, f2, f1, d_qpe));
+                CK(taylor_expansion_contribution(m + 1, 0.5 * dt, nwf, f1, f3, f2, nthreads));
+            }
+            CK(normalize_wf(nwf, f3, nthreads));
+            CK(DERIVS(f3, sg));
+            CK(DENSW(f3, sg));
+            if (sg) CK(density_caculate_tau(d_dens, nthreads));
+            CK(compute_potentials(0, d_dens, d_pots, 1.0, nthreads));
+            HKF_ALPHA();
+            CK(DERIVS(d_wf, sg));
+            ALAP(d_wf);
+            CK(HAPPLYW(0, d_wf, f1, NULL));
+            CK(cudaMemcpy(d_qpe, d_work, nwf * sizeof(double), cudaMemcpyDeviceToDevice));
+            CK(taylor_expansion_contribution(1, dt, nwf, f1, d_wf, f2, nthreads));
+            for (int m = 1; m < iters; m++) {
+                CK(DERIVS(f2, sg));
+                ALAP(f2);
+                CK(HAPPLYW(0, f2, f1, d_qpe));
+                CK(taylor_expansion_contribution(m + 1, dt, nwf, f1, d_wf, f2, nthreads));
+            }
+            CK(normalize_wf(nwf, d_wf, nthreads));
+        }
+        for (int h = 0; h < q; h++) CK(cudaMemcpy(d_f[h], rec + (size_t)h * M, M * sizeof(Z), cudaMemcpyDeviceToDevice));
+        cudaFree(rec);
+        cudaFree(d_qpe);
+        grads = 1;
+        CK(compute_derivatives(2 * nwf, d_wf, d_dx, d_dy, d_dz, d_lap, nthreads));
+        CK(DENS(grads));
+        CK(density_caculate_tau(d_dens, nthreads));
+        CK(compute_potentials(it, d_dens, d_pots, 1.0, nthreads));
+    }
 
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0); cudaEventCreate(&e1);

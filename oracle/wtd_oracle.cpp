@@ -595,7 +595,7 @@ static void alpha_laplace(std::vector<Complex> &w)
 
 /* apply_hamiltonian (pca_kernels.cu:233-495, 674-848; cpca_kernels.cu:231-490;
  * ccpca_kernels.cu:209-448): out = (H - <H>) w.  out may alias the laplacian buffer. */
-static void apply_hamiltonian(int it, std::vector<Complex> &w, Complex *out)
+static void apply_hamiltonian(int it, std::vector<Complex> &w, Complex *out, const double *useqpe = nullptr)
 {
     wslda_potential P = pots_view(pots.data());
 #ifdef CURRENT_CORRECTIONS
@@ -742,17 +742,37 @@ static void apply_hamiltonian(int it, std::vector<Complex> &w, Complex *out)
 #pragma omp parallel for
     for (int n = 0; n < S; n++) {
         double e = 0.0;
-        for (int i = 0; i < N; i++) {
-            Complex p = std::conj(U(w, n)[i]) * out[(size_t)n * N + i] +
-                        std::conj(V(w, n)[i]) * out[(size_t)S * N + (size_t)n * N + i];
-            e += p.real() * WTD_DV;
+        if (useqpe) {
+            e = useqpe[n]; /* given energies (useqpe, pca_kernels.cu:806-833) */
+        } else {
+            for (int i = 0; i < N; i++) {
+                Complex p = std::conj(U(w, n)[i]) * out[(size_t)n * N + i] +
+                            std::conj(V(w, n)[i]) * out[(size_t)S * N + (size_t)n * N + i];
+                e += p.real() * WTD_DV;
+            }
+            qpe[n] = e;
         }
-        qpe[n] = e;
         for (int i = 0; i < N; i++) {
             out[(size_t)n * N + i] -= U(w, n)[i] * e;
             out[(size_t)S * N + (size_t)n * N + i] -= V(w, n)[i] * e;
         }
     }
+}
+
+/* the fields apply_hamiltonian filters in place before building H, at every call: V_a, V_b
+ * (pca_kernels.cu:700-704), delta (mode 2, :758-762), the A components with current
+ * corrections outside BdG (:791-795) */
+static void filter_h_fields()
+{
+    if (hkf_mode < 1) return;
+    wslda_potential P = pots_view(pots.data());
+    high_k_filter(P.V_a);
+    high_k_filter(P.V_b);
+    if (hkf_mode >= 2) high_k_filter_c(P.delta);
+#if defined(CURRENT_CORRECTIONS) && !defined(BDG_MODE)
+    double *A[6] = {P.A_a_x, P.A_a_y, P.A_a_z, P.A_b_x, P.A_b_y, P.A_b_z};
+    for (int k = 0; k < 6; k++) high_k_filter(A[k]);
+#endif
 }
 
 /* densities -> potentials block shared by both half steps (pca.c:1424-1457) */
@@ -770,19 +790,7 @@ static void half_step_densities(int it_next, int grads)
         high_k_filter(P.alpha_b);
     }
 #endif
-    /* the fields apply_hamiltonian filters in place before building H: V_a, V_b
-     * (pca_kernels.cu:700-704), delta (mode 2, :758-762), the A components with current
-     * corrections outside BdG (:791-795) */
-    if (hkf_mode >= 1) {
-        wslda_potential P = pots_view(pots.data());
-        high_k_filter(P.V_a);
-        high_k_filter(P.V_b);
-        if (hkf_mode >= 2) high_k_filter_c(P.delta);
-#if defined(CURRENT_CORRECTIONS) && !defined(BDG_MODE)
-        double *A[6] = {P.A_a_x, P.A_a_y, P.A_a_z, P.A_b_x, P.A_b_y, P.A_b_z};
-        for (int k = 0; k < 6; k++) high_k_filter(A[k]);
-#endif
-    }
+    filter_h_fields();
     alpha_laplace(y);
 }
 
@@ -904,6 +912,110 @@ int orc_steps(int nsteps)
     return 0;
 }
 
+/* Taylor self-start of the ABM history (pca.c:1086-1330, selfstart 1): each of the q first
+ * steps records (H - <H>) psi of its start state as the newest history entry, takes a half step
+ * exp(-i H dt/2) psi by a Taylor series of exp_iters terms to build midpoint potentials, then
+ * the full step exp(-i H_mid dt) psi the same way and renormalises.  Potentials and H use time
+ * index 0 throughout ("potential is constant during first steps"), and the time index does not
+ * advance.  Afterwards the history holds the recorded entries (f1 newest) and densities and
+ * potentials are recomputed at the current time index. */
+static void taylor_term(int order, double dt, const std::vector<Complex> &h, std::vector<Complex> &upd,
+                        std::vector<Complex> &contr)
+{
+    /* taylor_expansion_contribution (pca_kernels.cu:1032-1062): contr = h * (i t), upd += contr,
+     * t = -dt/order */
+    const double t = -1.0 * dt / (double)order;
+    for (size_t i = 0; i < h.size(); i++) {
+        Complex c = h[i] * Complex(0.0, t);
+        contr[i] = c;
+        upd[i] += c;
+    }
+}
+
+static void selfstart()
+{
+    const int q = NHIST;
+    const int iters = (NHIST == 3) ? 4 : 5;
+#ifdef FAST_CONST_EFFECTIVE_MASS_MODE
+    const int grads = 0;
+#else
+    const int grads = 1;
+#endif
+    const size_t M = (size_t)2 * S * N;
+    std::vector<Complex> f1(M), f2(M), f3(M);
+    std::vector<std::vector<Complex>> rec(q, std::vector<Complex>(M, Complex(0.0, 0.0)));
+    std::vector<double> qs(S);
+    for (int step = 0; step < q; step++) {
+        /* densities and potentials of the start state (time index 0) */
+        derivatives(y, grads);
+        calculate_densities(y, grads);
+        exchange_densities();
+        if (grads) density_tau();
+        compute_potentials(0);
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+        if (hkf_mode >= 1) {
+            wslda_potential P = pots_view(pots.data());
+            high_k_filter(P.alpha_a);
+            high_k_filter(P.alpha_b);
+        }
+#endif
+        alpha_laplace(y);
+        /* H psi of the start state, recorded as the newest history entry */
+        f3 = y;
+        filter_h_fields();
+        apply_hamiltonian(0, f3, f1.data());
+        qs = qpe;
+        for (int h = q - 1; h > 0; h--) rec[h] = rec[h - 1];
+        rec[0] = f1;
+        /* half step: f3 = exp(-i H dt/2) psi, Taylor series */
+        taylor_term(1, 0.5 * md.dt, f1, f3, f2);
+        for (int m = 1; m < iters; m++) {
+            derivatives(f2, grads);
+            alpha_laplace(f2);
+            filter_h_fields();
+            apply_hamiltonian(0, f2, f1.data(), qs.data());
+            taylor_term(m + 1, 0.5 * md.dt, f1, f3, f2);
+        }
+        normalize(f3);
+        /* midpoint densities and potentials */
+        derivatives(f3, grads);
+        calculate_densities(f3, grads);
+        exchange_densities();
+        if (grads) density_tau();
+        compute_potentials(0);
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+        if (hkf_mode >= 1) {
+            wslda_potential P = pots_view(pots.data());
+            high_k_filter(P.alpha_a);
+            high_k_filter(P.alpha_b);
+        }
+#endif
+        /* full step from the start state with the midpoint H */
+        derivatives(y, grads);
+        alpha_laplace(y);
+        filter_h_fields();
+        apply_hamiltonian(0, y, f1.data());
+        qs = qpe;
+        taylor_term(1, md.dt, f1, y, f2);
+        for (int m = 1; m < iters; m++) {
+            derivatives(f2, grads);
+            alpha_laplace(f2);
+            filter_h_fields();
+            apply_hamiltonian(0, f2, f1.data(), qs.data());
+            taylor_term(m + 1, md.dt, f1, y, f2);
+        }
+        normalize(y);
+    }
+    for (int h = 0; h < q; h++) fk[h] = rec[h];
+    /* densities and potentials of the new state at the current time index (pca.c:1315-1318) */
+    derivatives(y, 1);
+    calculate_densities(y, 1);
+    exchange_densities();
+    density_tau();
+    compute_potentials(it_global);
+    last_gradients = 1;
+}
+
 /* compute_energy (tdwslda_energy_generic.h:21-111 and the functional energy kernels) */
 int orc_energy(double *E)
 {
@@ -987,6 +1099,11 @@ int orc_get_history(int slot, double *out)
     return 0;
 }
 int orc_get_it(void) { return it_global; }
+int orc_selfstart(void)
+{
+    selfstart();
+    return 0;
+}
 int orc_set_high_k_filter(int mode, double mu, double T)
 {
     hkf_mode = mode; hkf_mu = mu; hkf_T = T;

@@ -54,6 +54,15 @@ HKF2_CASES = {
 }
 
 
+# Taylor self-start of the history (pca.c:1086-1330, selfstart 1) before the steps
+SS_CASES = {
+    "t2d_slda": (24, 3, 2, True),
+    "t1d_aslda": (24, 3, 2, True),
+    "c4_bdg2d": (16, 4, 1, False),
+    "c3_aslda3d": (8, 2, 1, False),
+}
+
+
 def hkf_params(proj, mode=1):
     emax = 0.5 * np.pi ** 2 / proj.dx ** 2
     return mode, HKF_FRACTIONS[0] * emax, HKF_FRACTIONS[1] * emax
@@ -113,14 +122,16 @@ def slim(rec, n):
     return rec
 
 
-def run_case(name, out_dir, hkf=0):
-    nwf, nsteps, nmeas, full = {0: CASES, 1: HKF_CASES, 2: HKF2_CASES}[hkf][name]
+def run_case(name, out_dir, hkf=0, selfstart=False):
+    nwf, nsteps, nmeas, full = (SS_CASES if selfstart else {0: CASES, 1: HKF_CASES, 2: HKF2_CASES}[hkf])[name]
     proj, y0, occ, pots, params, extra = case_inputs(name, nwf)
     so = os.path.join(REPO, "oracle", "_ref", name, "libref.so")
     lib = ctypes.CDLL(so, mode=ctypes.RTLD_LOCAL)
     lib.refh_set_hkf.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
     mode, mu, T = hkf_params(proj, hkf) if hkf else (0, 0.0, 1.0)
     lib.refh_set_hkf(mode, mu, T)
+    lib.refh_set_selfstart.argtypes = [ctypes.c_int]
+    lib.refh_set_selfstart(1 if selfstart else 0)
     lib.refh_numel.restype = ctypes.c_int
     lib.refh_nhist.restype = ctypes.c_int
     n = lib.refh_numel()
@@ -153,7 +164,7 @@ def run_case(name, out_dir, hkf=0):
     if hkf:
         rec["hkf"] = np.array([mode, mu, T])
     rec = slim(rec, n)
-    path = os.path.join(out_dir, f"{name}{fixture_suffix(hkf)}.npz")
+    path = os.path.join(out_dir, f"{name}{'_ss' if selfstart else fixture_suffix(hkf)}.npz")
     np.savez_compressed(path, **rec)
     print(f"{name}: nwf={nwf} steps={nsteps}x{nmeas} E={en[:7].sum():.12g} N={en[7]:.12g},{en[8]:.12g} "
           f"ms/step={ms[0]:.3f} -> {path}")
@@ -165,6 +176,7 @@ def main():
     ap.add_argument("--slim-existing", action="store_true", help="apply slim() to fixtures in --out")
     ap.add_argument("--hkf", type=int, default=0, choices=[0, 1, 2],
                     help="1: the effective-mass filter cases (HKF_CASES); 2: masses and pairing field (HKF2_CASES)")
+    ap.add_argument("--selfstart", action="store_true", help="the Taylor self-start cases (SS_CASES)")
     ap.add_argument("projects", nargs="*")
     a = ap.parse_args()
     if a.slim_existing:
@@ -177,8 +189,9 @@ def main():
                     np.savez_compressed(path, **slim(rec, n))
         return
     os.makedirs(a.out, exist_ok=True)
-    for name in (a.projects or list({0: CASES, 1: HKF_CASES, 2: HKF2_CASES}[a.hkf])):
-        run_case(name, a.out, hkf=a.hkf)
+    table = SS_CASES if a.selfstart else {0: CASES, 1: HKF_CASES, 2: HKF2_CASES}[a.hkf]
+    for name in (a.projects or list(table)):
+        run_case(name, a.out, hkf=a.hkf, selfstart=a.selfstart)
 
 
 if __name__ == "__main__":

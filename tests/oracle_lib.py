@@ -58,6 +58,7 @@ class Oracle:
         L.orc_derivatives_field.argtypes = [_dp] * 5
         L.orc_set_density_exchange.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.orc_set_high_k_filter.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.orc_selfstart.restype = ctypes.c_int
         L.orc_filter_field.argtypes = [_dp]
         self._xfn = None
         # the library is shared by every instance in the process: start from a plain run
@@ -85,6 +86,9 @@ class Oracle:
 
     def initial_measurement(self):
         return self.lib.orc_initial_measurement()
+
+    def selfstart(self):
+        return self.lib.orc_selfstart()
 
     def set_high_k_filter(self, mode, mu, T):
         self.lib.orc_set_high_k_filter(int(mode), float(mu), float(T))

@@ -17,7 +17,7 @@ def inputs(name, nwf, seed_salt=0):
     return proj, dict(states=y0, pots=pots, occ=occ, params=params, extra=extra)
 
 
-def run_oracle(name, nwf, nsteps, nmeas=1, inp=None, threads=None, hkf=None):
+def run_oracle(name, nwf, nsteps, nmeas=1, inp=None, threads=None, hkf=None, selfstart=False):
     from oracle_lib import Oracle
     proj, d = inputs(name, nwf) if inp is None else (P.Project(name), inp)
     o = Oracle(name, threads=threads)
@@ -25,13 +25,15 @@ def run_oracle(name, nwf, nsteps, nmeas=1, inp=None, threads=None, hkf=None):
         o.set_high_k_filter(*hkf)
     o.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
     o.initial_measurement()
+    if selfstart:
+        o.selfstart()
     for _ in range(nmeas):
         o.steps(nsteps)
     return dict(states=o.states(), densities=o.densities(), potentials=o.potentials(), energy=o.energy(),
                 qpe=o.qpe(), history=[o.history(s) for s in range(proj.nhist)])
 
 
-def run_gpu(name, nwf, nsteps, nmeas=1, precision=0, inp=None, hkf=None):
+def run_gpu(name, nwf, nsteps, nmeas=1, precision=0, inp=None, hkf=None, selfstart=False):
     from wslda_b200 import TDRun
     proj, d = inputs(name, nwf) if inp is None else (P.Project(name), inp)
     r = TDRun(name, nwf, precision=precision)
@@ -39,6 +41,8 @@ def run_gpu(name, nwf, nsteps, nmeas=1, precision=0, inp=None, hkf=None):
         r.set_high_k_filter(*hkf)
     r.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
     r.initial_measurement()
+    if selfstart:
+        r.selfstart()
     for _ in range(nmeas):
         r.steps(nsteps)
     out = dict(states=r.states(), densities=r.densities(), potentials=r.potentials(), energy=r.energy(),

@@ -87,3 +87,19 @@ def test_t2d_big_staged(has_gpu):
     """2D 160x96 ASLDA: a radix-5 axis longer than 128 points and a state too large for one
     CTA, so the 2D plane/pencil path"""
     _compare("t2d_big", nwf=8, nsteps=3, nmeas=1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,nwf,nsteps,nmeas", [("t2d_slda", 24, 3, 2), ("t1d_aslda", 24, 3, 2), ("c4_bdg2d", 16, 4, 1),
+                                                   ("c3_aslda3d", 8, 2, 1), ("t2d_vext", 24, 3, 1)])
+def test_selfstart(has_gpu, name, nwf, nsteps, nmeas):
+    """Taylor self-start of the history (pca.c:1086-1330) then the ABM steps: constant and
+    variable mass, 1D/2D/3D, fused and plane/pencil lattices"""
+    o = run_oracle(name, nwf, nsteps, nmeas, selfstart=True)
+    g = run_gpu(name, nwf, nsteps, nmeas, selfstart=True)
+    n = o["densities"].size // 12
+    for k, v in density_errors(g["densities"], o["densities"], n).items():
+        assert v < TOL, f"{name} density {k}: rel err {v:.3e}"
+    assert rel(g["potentials"], o["potentials"]) < TOL
+    assert rel(g["states"], o["states"]) < TOL
+    assert rel(g["history0"], o["history"][0]) < TOL

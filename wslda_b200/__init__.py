@@ -39,6 +39,7 @@ SIGNATURES = {
     "wtd_download_history": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "wtd_initial_measurement": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "wtd_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "wtd_selfstart": (ctypes.c_int, [ctypes.c_void_p]),
     "wtd_energy": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "wtd_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "wtd_time_index": (ctypes.c_int, [ctypes.c_void_p]),
@@ -139,6 +140,10 @@ class TDRun:
 
     def initial_measurement(self, it0=None):
         self._check(self.lib.wtd_initial_measurement(self.h, int(self.it0 if it0 is None else it0)))
+
+    def selfstart(self):
+        """Taylor self-start of the ABM history (after initial_measurement)"""
+        self._check(self.lib.wtd_selfstart(self.h))
 
     def steps(self, n):
         self._check(self.lib.wtd_steps(self.h, int(n)))

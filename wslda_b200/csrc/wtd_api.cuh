@@ -195,46 +195,95 @@ static int ensure_fk(wtd_ctx *c)
     return WTD_OK;
 }
 
-/* high-k filters of the fields H is built from, once after every functional evaluation, as
- * the reference does (in place) between compute_potentials and the H application:
- *   hkf_mode >= 1: alpha_a, alpha_b in variable-mass runs (driver, pca.c:1448-1453), V_a, V_b
- *                  (apply_hamiltonian, pca_kernels.cu:700-704) and, with current corrections
- *                  outside BdG, the six A components (pca_kernels.cu:791-795);
- *   hkf_mode >= 2: also the pairing field (pca_kernels.cu:758-762) */
-static int filter_fields(wtd_ctx *c)
+/* high-k filters (hkf_mode) of the fields H is built from, in place, f -> IFFT[FD FFT f]:
+ *   filter_alpha: alpha_a, alpha_b in variable-mass runs, after each functional evaluation
+ *                 (the driver, pca.c:1448-1453; hkf_mode >= 1);
+ *   filter_h:     V_a, V_b (hkf_mode >= 1, pca_kernels.cu:700-704), the pairing field (>= 2,
+ *                 :758-762) and, with current corrections outside BdG, the six A components
+ *                 (>= 1, :791-795) — the reference filters these at the top of every
+ *                 apply_hamiltonian, which a step calls once after each functional evaluation */
+static int filter_real(wtd_ctx *c, double *f, int nf)
+{
+    constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
+    if (WTD_BIG) return big_filter_real(f, nf, c->hkf_mu, c->hkf_T, c->stage3d, c->tw, c->ktab, c->st);
+    if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+    static bool attr = false;
+    if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_hkf_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+    wtd_hkf_kernel<WG><<<nf, 512, sm, c->st>>>(f, c->hkf_mu, c->hkf_T, c->tw, c->ktab);
+    WTD_LAUNCHED(c);
+    return WTD_OK;
+}
+
+static int filter_alpha(wtd_ctx *c)
+{
+    if (c->hkf_mode < 1 || !WTD_VAR) return WTD_OK;
+    return filter_real(c, c->pots + 4 * (size_t)WTD_NUMEL, 2);
+}
+
+static int filter_h(wtd_ctx *c)
 {
     if (c->hkf_mode < 1) return WTD_OK;
     constexpr size_t N = WTD_NUMEL;
-    constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
-    struct { double *f; int nf; } real[3] = {{c->pots, 2}, {NULL, 0}, {NULL, 0}};   /* V_a, V_b */
-    if (WTD_VAR) real[1] = {c->pots + 4 * N, 2};                                    /* alpha_a, alpha_b */
+    WTD_TRY(filter_real(c, c->pots, 2));
 #if defined(CURRENT_CORRECTIONS) && !defined(BDG_MODE)
-    real[2] = {c->pots + 6 * N, 6};                                                 /* A_a xyz, A_b xyz */
+    WTD_TRY(filter_real(c, c->pots + 6 * N, 6));
 #endif
-    double2 *delta = (double2 *)(c->pots + 2 * N);
-    if (WTD_BIG) {
-        for (int k = 0; k < 3; k++)
-            if (real[k].f) WTD_TRY(big_filter_real(real[k].f, real[k].nf, c->hkf_mu, c->hkf_T, c->stage3d, c->tw, c->ktab, c->st));
-        if (c->hkf_mode >= 2)
-            WTD_TRY(big_derivs(delta, 1, delta, NULL, NULL, NULL, c->tw, c->ktab, c->st, 1, c->hkf_mu, c->hkf_T));
-        return WTD_OK;
-    }
-    if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
-    static bool attr = false;
-    if (!attr) {
-        WTD_CU(cudaFuncSetAttribute(wtd_hkf_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        WTD_CU(cudaFuncSetAttribute(wtd_hkf_c_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        attr = true;
-    }
-    for (int k = 0; k < 3; k++)
-        if (real[k].f) {
-            wtd_hkf_kernel<WG><<<real[k].nf, 512, sm, c->st>>>(real[k].f, c->hkf_mu, c->hkf_T, c->tw, c->ktab);
-            WTD_LAUNCHED(c);
-        }
     if (c->hkf_mode >= 2) {
+        double2 *delta = (double2 *)(c->pots + 2 * N);
+        if (WTD_BIG) return big_derivs(delta, 1, delta, NULL, NULL, NULL, c->tw, c->ktab, c->st, 1, c->hkf_mu, c->hkf_T);
+        constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
+        if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+        static bool attr = false;
+        if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_hkf_c_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
         wtd_hkf_c_kernel<WG><<<1, 512, sm, c->st>>>(delta, delta, c->hkf_mu, c->hkf_T, c->tw, c->ktab);
         WTD_LAUNCHED(c);
     }
+    return WTD_OK;
+}
+
+static int filter_fields(wtd_ctx *c)
+{
+    WTD_TRY(filter_alpha(c));
+    return filter_h(c);
+}
+
+/* per-point H coefficients from the potentials at time index it (variable mass: lap alpha /4
+ * and -div A /2 by spectral derivatives) */
+static int coef_from_pots(wtd_ctx *c, int it)
+{
+    constexpr int N = WTD_NUMEL;
+    wslda_potential P = convert_into_wslda_potential(c->pots, N, NULL);
+    wtd_prep_coef<<<(N + 127) / 128, 128, 0, c->st>>>(it, P, c->cf);
+    WTD_LAUNCHED(c);
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+    if (WTD_BIG) {
+        WTD_TRY(big_prep_var(c->cf, c->stage3d, c->tw, c->ktab, c->st));
+    } else {
+        constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
+        if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+        static bool attr = false;
+        if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_prep_var<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+        wtd_prep_var<WG><<<2, 256, sm, c->st>>>(c->cf, c->tw, c->ktab);
+        WTD_LAUNCHED(c);
+    }
+#endif
+    c->have_coef = 1;
+    return WTD_OK;
+}
+
+/* the functional at time index it (potentials kernel and the user's modify_potentials) */
+static int functional(wtd_ctx *c, int it)
+{
+    constexpr int N = WTD_NUMEL;
+    wslda_density D = convert_into_wslda_density(c->dens, N);
+    wslda_potential P = convert_into_wslda_potential(c->pots, N, NULL);
+    int pb = (N + 127) / 128;
+    wtd_potentials_kernel<<<pb, 128, 0, c->st>>>(it, D, P, 1.0);
+    WTD_LAUNCHED(c);
+#ifdef ENABLE_MODIFY_POTENTIALS
+    modify_potentials<<<pb, 128, 0, c->st>>>(it, D, P);
+    WTD_LAUNCHED(c);
+#endif
     return WTD_OK;
 }
 
@@ -255,30 +304,9 @@ static int after_pass(wtd_ctx *c, bool full, int it)
         WTD_LAUNCHED(c);
     }
     if (it < 0) return WTD_OK;
-    wslda_density D = convert_into_wslda_density(c->dens, N);
-    wslda_potential P = convert_into_wslda_potential(c->pots, N, NULL);
-    int pb = (N + 127) / 128;
-    wtd_potentials_kernel<<<pb, 128, 0, c->st>>>(it, D, P, 1.0);
-    WTD_LAUNCHED(c);
-#ifdef ENABLE_MODIFY_POTENTIALS
-    modify_potentials<<<pb, 128, 0, c->st>>>(it, D, P);
-    WTD_LAUNCHED(c);
-#endif
+    WTD_TRY(functional(c, it));
     WTD_TRY(filter_fields(c));
-    wtd_prep_coef<<<pb, 128, 0, c->st>>>(it, P, c->cf);
-    WTD_LAUNCHED(c);
-#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
-    {
-        constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
-        if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
-        static bool attr = false;
-        if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_prep_var<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
-        wtd_prep_var<WG><<<2, 256, sm, c->st>>>(c->cf, c->tw, c->ktab);
-        WTD_LAUNCHED(c);
-    }
-#endif
-    c->have_coef = 1;
-    return WTD_OK;
+    return coef_from_pots(c, it);
 }
 
 /* ---------------------------------------------------------------------------------------
@@ -961,6 +989,191 @@ int wtd_set_density_exchange(wtd_ctx *c, wtd_exchange_fn fn, void *user)
 }
 
 } /* extern "C" */
+
+/* ---------------------------------------------------------------------------------------
+ * Taylor self-start of the ABM history (pca.c:1086-1330, input selfstart 1), FP64: the q
+ * first steps are taken with exp(-i H dt) expanded to exp_iters orders (midpoint potentials
+ * from a half step), recording (H - <H>) psi of each start state as the history, so that the
+ * predictor-corrector starts from a consistent history instead of the zero one.  The
+ * reference keeps the time index at its start value and evaluates potentials and H at time
+ * index 0 during these steps; so does this.
+ * -------------------------------------------------------------------------------------*/
+struct SelfWork {
+    double2 *ddx, *ddy, *ddz, *dlap, *dalap, *rec;
+    double *qs;
+    std::vector<void *> own;
+};
+
+static int ss_derivs(wtd_ctx *c, SelfWork &w, const double2 *in, int grads)
+{
+    const int nf = 2 * c->S;
+    double2 *dx = grads ? w.ddx : NULL, *dy = (grads && CODEDIM >= 2) ? w.ddy : NULL, *dz = (grads && CODEDIM >= 3) ? w.ddz : NULL;
+    if (WTD_BIG) return big_derivs((double2 *)in, nf, w.dlap, dx, dy, dz, c->tw, c->ktab, c->st);
+    if (k_derivs_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+    static bool attr = false;
+    if (!attr) { WTD_CU(cudaFuncSetAttribute(k_derivs<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k_derivs_smem)); attr = true; }
+    k_derivs<WG><<<nf, 512, k_derivs_smem, c->st>>>(in, dx, dy, dz, w.dlap, c->tw, c->ktab);
+    WTD_LAUNCHED(c);
+    return WTD_OK;
+}
+
+/* densities of the states in `in` (derivatives from ss_derivs), summed over ranks, tau */
+static int ss_densities(wtd_ctx *c, SelfWork &w, const double2 *in, int grads)
+{
+    constexpr int N = WTD_NUMEL;
+    k_dens_compat<<<c->grid, 256, 0, c->st>>>(c->S, in, w.ddx, w.ddy, w.ddz, w.dlap, c->occ, NULL, c->kp2, c->wcnt,
+                                              c->dslot, grads);
+    WTD_LAUNCHED(c);
+    wtd_dens_reduce<<<(12 * N + 255) / 256, 256, 0, c->st>>>(c->dslot, c->grid, c->dens, N, grads, 1.0 / WTD_LPERP);
+    WTD_LAUNCHED(c);
+    WTD_TRY(exchange(c, c->dens, 12 * (size_t)N));
+    if (!grads) return WTD_OK;
+    if (WTD_BIG) return big_tau(c->dens, c->stage3d, c->tw, c->ktab, c->st);
+    constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
+    static bool attr = false;
+    if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_tau_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+    wtd_tau_kernel<WG><<<2, 512, sm, c->st>>>(c->dens, c->tw, c->ktab);
+    WTD_LAUNCHED(c);
+    return WTD_OK;
+}
+
+/* lap(alpha psi) for the variable-mass kinetic term (multiply_wf_by_alpha + compute_laplace) */
+static int ss_alap(wtd_ctx *c, SelfWork &w, const double2 *in)
+{
+#ifndef FAST_CONST_EFFECTIVE_MASS_MODE
+    constexpr size_t N = WTD_NUMEL;
+    const size_t M = (size_t)2 * c->S * N;
+    k_mul_alpha<<<(unsigned)((M + 255) / 256), 256, 0, c->st>>>(c->S, in, w.dalap, c->pots + 4 * N, c->pots + 5 * N);
+    WTD_LAUNCHED(c);
+    if (WTD_BIG) return big_derivs(w.dalap, 2 * c->S, w.dalap, NULL, NULL, NULL, c->tw, c->ktab, c->st);
+    k_derivs<WG><<<2 * c->S, 512, k_derivs_smem, c->st>>>(w.dalap, NULL, NULL, NULL, w.dalap, c->tw, c->ktab);
+    WTD_LAUNCHED(c);
+#else
+    (void)c; (void)w; (void)in;
+#endif
+    return WTD_OK;
+}
+
+/* out = (H - E) in at time index 0; E computed into c->qpe, or the given useqpe.  The
+ * fields are filtered first, as at the top of every apply_hamiltonian of the reference. */
+static int ss_hamiltonian(wtd_ctx *c, SelfWork &w, const double2 *in, double2 *out, const double *useqpe)
+{
+    WTD_TRY(filter_h(c));
+    WTD_TRY(coef_from_pots(c, 0));
+    k_hamiltonian_compat<<<c->S, 256, 0, c->st>>>(c->S, in, out, w.ddx, w.ddy, w.ddz, w.dlap, w.dalap, c->cf, c->kp2,
+                                                  c->qpe, useqpe);
+    WTD_LAUNCHED(c);
+    return WTD_OK;
+}
+
+/* the Taylor order `order` of exp(-i H t): contr = (i t/order) h, upd += contr */
+static int ss_taylor(wtd_ctx *c, const double2 *h, double2 *upd, double2 *contr, double t, int order)
+{
+    const size_t M = (size_t)2 * c->S * WTD_NUMEL;
+    k_taylor<<<(unsigned)((M + 255) / 256), 256, 0, c->st>>>(M, h, upd, contr, -1.0 * t / (double)order);
+    WTD_LAUNCHED(c);
+    return WTD_OK;
+}
+
+static int selfstart_run(wtd_ctx *c, SelfWork &w)
+{
+    constexpr int NH = WTD_NHIST;
+    constexpr size_t N = WTD_NUMEL;
+    const int q = NH, iters = (NH == 3) ? 4 : 5;
+    const int grads = WTD_VAR ? 1 : 0;
+    const size_t NS = (size_t)2 * c->S * N, bytes = NS * sizeof(double2);
+    double2 *y = (double2 *)c->y;
+    /* work arrays: the physical history slots, overwritten by the history at the end */
+    double2 *f1 = (double2 *)c->hist[0], *f2 = (double2 *)c->hist[1], *f3 = (double2 *)c->hist[2];
+    const double dt = c->dt;
+    for (int step = 0; step < q; step++) {
+        /* start state: densities and potentials at time index 0, its (H - <H>) psi recorded */
+        WTD_TRY(ss_derivs(c, w, y, grads));
+        WTD_TRY(ss_densities(c, w, y, grads));
+        WTD_TRY(functional(c, 0));
+        WTD_TRY(filter_alpha(c));
+        WTD_TRY(ss_alap(c, w, y));
+        WTD_CU(cudaMemcpyAsync(f3, y, bytes, cudaMemcpyDeviceToDevice, c->st));
+        WTD_TRY(ss_hamiltonian(c, w, f3, f1, NULL));
+        WTD_CU(cudaMemcpyAsync(w.qs, c->qpe, c->S * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+        for (int h = q - 1; h > 0; h--)
+            WTD_CU(cudaMemcpyAsync(w.rec + h * NS, w.rec + (h - 1) * NS, bytes, cudaMemcpyDeviceToDevice, c->st));
+        WTD_CU(cudaMemcpyAsync(w.rec, f1, bytes, cudaMemcpyDeviceToDevice, c->st));
+        /* half step into f3 */
+        WTD_TRY(ss_taylor(c, f1, f3, f2, 0.5 * dt, 1));
+        for (int m = 1; m < iters; m++) {
+            WTD_TRY(ss_derivs(c, w, f2, grads));
+            WTD_TRY(ss_alap(c, w, f2));
+            WTD_TRY(ss_hamiltonian(c, w, f2, f1, w.qs));
+            WTD_TRY(ss_taylor(c, f1, f3, f2, 0.5 * dt, m + 1));
+        }
+        k_normalize<<<c->S, 256, 0, c->st>>>(c->S, f3);
+        WTD_LAUNCHED(c);
+        /* midpoint potentials */
+        WTD_TRY(ss_derivs(c, w, f3, grads));
+        WTD_TRY(ss_densities(c, w, f3, grads));
+        WTD_TRY(functional(c, 0));
+        WTD_TRY(filter_alpha(c));
+        /* full step of the state with the midpoint H */
+        WTD_TRY(ss_derivs(c, w, y, grads));
+        WTD_TRY(ss_alap(c, w, y));
+        WTD_TRY(ss_hamiltonian(c, w, y, f1, NULL));
+        WTD_CU(cudaMemcpyAsync(w.qs, c->qpe, c->S * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+        WTD_TRY(ss_taylor(c, f1, y, f2, dt, 1));
+        for (int m = 1; m < iters; m++) {
+            WTD_TRY(ss_derivs(c, w, f2, grads));
+            WTD_TRY(ss_alap(c, w, f2));
+            WTD_TRY(ss_hamiltonian(c, w, f2, f1, w.qs));
+            WTD_TRY(ss_taylor(c, f1, y, f2, dt, m + 1));
+        }
+        k_normalize<<<c->S, 256, 0, c->st>>>(c->S, y);
+        WTD_LAUNCHED(c);
+    }
+    /* the recorded entries become the history, f1 (newest) the given f_k of the next step */
+    void *slot[WTD_NHIST];
+    ring_slots(c, slot);
+    for (int r = 0; r < q; r++)
+        WTD_CU(cudaMemcpyAsync(slot[ring_of_ref_slot(r)], w.rec + r * NS, bytes, cudaMemcpyDeviceToDevice, c->st));
+    c->fk_given = 1;
+    /* densities and potentials of the new state at the current time index (pca.c:1315-1318) */
+    WTD_TRY(ss_derivs(c, w, y, 1));
+    WTD_TRY(ss_densities(c, w, y, 1));
+    WTD_TRY(functional(c, c->it));
+    return coef_from_pots(c, c->it);
+}
+
+extern "C" int wtd_selfstart(wtd_ctx *c)
+{
+    if (!c) return WTD_ERR_ARG;
+    if (c->prec != WTD_FP64) return WTD_ERR_UNSUPPORTED;
+    WTD_CU(cudaSetDevice(c->dev));
+    constexpr size_t N = WTD_NUMEL;
+    const size_t NS = (size_t)2 * c->S * N;
+    SelfWork w{};
+    auto get = [&](double2 **p, size_t n) -> int {
+        void *q = NULL;
+        if (cudaMalloc(&q, n * sizeof(double2)) != cudaSuccess) { cudaGetLastError(); return WTD_ERR_NOMEM; }
+        w.own.push_back(q);
+        *p = (double2 *)q;
+        return WTD_OK;
+    };
+    int r = WTD_OK;
+    if (c->staged) {
+        w.ddx = c->ddx; w.ddy = c->ddy; w.ddz = c->ddz; w.dlap = c->dlap; w.dalap = c->dalap;
+    } else {
+        r = get(&w.ddx, NS);
+        if (!r && CODEDIM >= 2) r = get(&w.ddy, NS);
+        if (!r && CODEDIM >= 3) r = get(&w.ddz, NS);
+        if (!r) r = get(&w.dlap, NS);
+        if (!r && WTD_VAR) r = get(&w.dalap, NS);
+    }
+    if (!r) r = get(&w.rec, (size_t)WTD_NHIST * NS);
+    if (!r) r = get((double2 **)&w.qs, (size_t)c->S);
+    if (!r) r = selfstart_run(c, w);
+    cudaStreamSynchronize(c->st);
+    for (void *q : w.own) cudaFree(q);
+    return r ? r : wtd_cuerr(cudaGetLastError());
+}
 
 /* ---------------------------------------------------------------------------------------
  * adjoint (gradient of a loss of the final pairing field with respect to the parameters of
