@@ -89,6 +89,19 @@ int calculate_densities(int n, wtd_z *wf, wtd_z *wf_d_dx, wtd_z *wf_d_dy, wtd_z 
 int calculate_densities(int n, wtd_z *wf, wtd_z *wf_d_dx, wtd_z *d_wf_laplace, double *kkyz,
                         double *d_fbetaEn, double *weights, int *cnt, double *d_densities, int gradients_computed, int nthreads);
 #endif
+/* quantum-friction densities [U_a, U_b, D (complex)] (4 N doubles; the reference keeps them at
+ * d_densities + 12 N) from the states and their laplacians (hpc-engine/pca_dens.cu:431,
+ * cpca_dens.cu:471, ccpca_dens.cu:470); apply_hamiltonian reads them there when qfswitch > 0 */
+#if WTD_CODEDIM == 3
+int calculate_quantum_friction_densities(int n, wtd_z *wf, wtd_z *d_wf_laplace, double *d_fbetaEn, double *weights,
+                                         double *d_qf_densities, int nthreads);
+#elif WTD_CODEDIM == 2
+int calculate_quantum_friction_densities(int n, wtd_z *wf, wtd_z *d_wf_laplace, double *kkz, double *d_fbetaEn,
+                                         double *weights, double *d_qf_densities, int nthreads);
+#else
+int calculate_quantum_friction_densities(int n, wtd_z *wf, wtd_z *d_wf_laplace, double *kkyz, double *d_fbetaEn,
+                                         double *weights, int *cnt, double *d_qf_densities, int nthreads);
+#endif
 #define WTD_ERR_NOALLOC_SIZE -6
 /* calculate_densities_noalloc: no counterpart in the reference.  Same arguments, result and
  * error behaviour as calculate_densities above, for callers that cannot call cudaMalloc (a

@@ -142,6 +142,15 @@ int wtd_adjoint_release(wtd_ctx *ctx);
  * of E_max = pi^2 / (2 dx^2), pca.c:183-185); mode 0 turns filtering off. */
 int wtd_set_high_k_filter(wtd_ctx *ctx, int mode, double mu, double T);
 
+/* quantum friction (cooling), as the reference's input qfalpha, qfbeta, qfgamma, qfNreq,
+ * qfstart, qfstop, qfswitch (the times in units of 1/eF): in every step whose switch
+ * (pca_utils.c:779-790, 1055-1060) is on, the friction densities are accumulated with the
+ * gradient densities and H is built from V_s - U_s alpha/nF and the phase and particle-control
+ * corrections of delta (pca_kernels.cu:497-539); the potentials themselves are not changed.
+ * All coefficients 0 turns it off.  Fused-path lattices only (WTD_ERR_UNSUPPORTED otherwise). */
+int wtd_set_quantum_friction(wtd_ctx *ctx, double qfalpha, double qfbeta, double qfgamma, double qfNreq,
+                             double qfstart, double qfstop, double qfswitch);
+
 /* ---- state-sharded runs (one process per GPU, each context holding a block of the states) ----
  * Densities are sums over states, so every density reduction of a sharded run is followed by a
  * sum over ranks: the reference's MPI_Allreduce of d_densities (hpc-engine/pca.c:948, 1433,

@@ -96,6 +96,45 @@ extern "C" int refh_set_selfstart(int on)
     return 0;
 }
 
+/* quantum friction (pca.c:1405-1430, 1458): coefficients and switch times as the input gives
+ * them (times in 1/eF), off unless set */
+static double qf_par[7] = {0, 0, 0, 0, 0, 0, 0}; /* alpha, beta, gamma, Nreq, start, stop, ramp */
+extern "C" int refh_set_quantum_friction(double alpha, double beta, double gamma, double nreq, double start, double stop,
+                                         double ramp)
+{
+    qf_par[0] = alpha; qf_par[1] = beta; qf_par[2] = gamma; qf_par[3] = nreq;
+    qf_par[4] = start; qf_par[5] = stop; qf_par[6] = ramp;
+    return 0;
+}
+/* volume element of the particle-number integral (pca.c:1458; cpca.c:1323; ccpca.c:1200) */
+#if REF_CODEDIM == 3
+#define REF_VOLEL (DX * DY * DZ)
+#elif REF_CODEDIM == 2
+#define REF_VOLEL (DX * DY * (NZ * DZ))
+#else
+#define REF_VOLEL (DX * (NY * DY) * (NZ * DZ))
+#endif
+/* the smooth switch of the input's qfstart/qfstop/qfswitch times (restated, pca_utils.c:779-790) */
+static double hr_ramp(double s, double ramp) { return 0.5 * (1.0 + tanh(tan(M_PI_2 * (2.0 * s / ramp - 1.0)))); }
+static double hr_switch(double t, double eF)
+{
+    if (qf_par[0] == 0.0 && qf_par[1] == 0.0 && qf_par[2] == 0.0) return 0.0;
+    const double a = qf_par[4] / eF, b = qf_par[5] / eF, r = qf_par[6] / eF;
+    if (t <= a || t >= b) return 0.0;
+    if (t >= a + r && t <= b - r) return 1.0;
+    if (t > a && t < a + r) return hr_ramp(t - a, r);
+    return 1.0 - hr_ramp(t - b + r, r);
+}
+extern "C" {
+#if REF_CODEDIM == 3
+int calculate_quantum_friction_densities(int n, Z *wf, Z *lap, double *fb, double *w, double *qf, int nthreads);
+#elif REF_CODEDIM == 2
+int calculate_quantum_friction_densities(int n, Z *wf, Z *lap, double *kkz, double *fb, double *w, double *qf, int nthreads);
+#else
+int calculate_quantum_friction_densities(int n, Z *wf, Z *lap, double *kkyz, double *fb, double *w, int *cnt, double *qf, int nthreads);
+#endif
+}
+
 /* effective-mass filtering of the reference driver (pca.c:1448-1453), off unless set */
 static int hkf_mode = 0;
 static double hkf_mu = 0.0, hkf_T = 1.0;
@@ -122,6 +161,7 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
     md.sclgth = sclgth;
     md.ec = ec;
     md.dt = dt;
+    md.qfalpha = qf_par[0]; md.qfbeta = qf_par[1]; md.qfgamma = qf_par[2]; md.qfNreq = qf_par[3];
     md.hkf_mode = hkf_mode; /* apply_hamiltonian reads it for the pairing-field filter */
     md.hkf_mu = hkf_mu;
     md.hkf_T = hkf_T;
@@ -182,13 +222,16 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
     /* dimension-dependent call shapes */
 #if REF_CODEDIM == 3
 #define DENSW(w, g) calculate_densities(nwf, w, d_dx, d_dy, d_dz, d_lap, d_fb, NULL, d_dens, g, nthreads)
-#define HAPPLYW(it, in, out, uq) apply_hamiltonian(it, nwf, in, out, d_dx, d_dy, d_dz, d_lap, d_alap, d_dens, d_pots, 0.0, uq, 0.0, nthreads)
+#define HAPPLYW(it, in, out, uq) apply_hamiltonian(it, nwf, in, out, d_dx, d_dy, d_dz, d_lap, d_alap, d_dens, d_pots, qfsw, uq, pcc, nthreads)
+#define QFDENS() calculate_quantum_friction_densities(nwf, d_wf, d_lap, d_fb, NULL, d_dens + 12 * (size_t)RN, nthreads)
 #elif REF_CODEDIM == 2
 #define DENSW(w, g) calculate_densities(nwf, w, d_dx, d_dy, d_lap, d_kk, d_fb, NULL, d_dens, g, nthreads)
-#define HAPPLYW(it, in, out, uq) apply_hamiltonian(it, nwf, in, out, d_dx, d_dy, d_kk, d_lap, d_alap, d_dens, d_pots, 0.0, uq, 0.0, nthreads)
+#define HAPPLYW(it, in, out, uq) apply_hamiltonian(it, nwf, in, out, d_dx, d_dy, d_kk, d_lap, d_alap, d_dens, d_pots, qfsw, uq, pcc, nthreads)
+#define QFDENS() calculate_quantum_friction_densities(nwf, d_wf, d_lap, d_kk, d_fb, NULL, d_dens + 12 * (size_t)RN, nthreads)
 #else
 #define DENSW(w, g) calculate_densities(nwf, w, d_dx, d_lap, d_kk, d_fb, NULL, d_cnt, d_dens, g, nthreads)
-#define HAPPLYW(it, in, out, uq) apply_hamiltonian(it, nwf, in, out, d_dx, d_kk, d_lap, d_alap, d_dens, d_pots, 0.0, uq, 0.0, nthreads)
+#define HAPPLYW(it, in, out, uq) apply_hamiltonian(it, nwf, in, out, d_dx, d_kk, d_lap, d_alap, d_dens, d_pots, qfsw, uq, pcc, nthreads)
+#define QFDENS() calculate_quantum_friction_densities(nwf, d_wf, d_lap, d_kk, d_fb, NULL, d_cnt, d_dens + 12 * (size_t)RN, nthreads)
 #endif
 #define DENS(g) DENSW(d_wf, g)
 #define HAPPLY(it, out) HAPPLYW(it, d_wf, out, NULL)
@@ -203,6 +246,21 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
 
     int it = it0;
     int grads = 1;
+    double qfsw = 0.0, pcc = 0.0;
+    const double eF_run = 0.5 * kF * kF;
+    /* (N - N_req) / N_req with N_req kept >= 1 (the reference's intent, pca_utils.c:1063-1072) */
+    auto host_pccoeff = [&]() -> double {
+        double *h = (double *)malloc(2 * RN * sizeof(double));
+        cudaMemcpy(h, d_dens + 2 * (size_t)RN, RN * sizeof(double), cudaMemcpyDeviceToHost);
+        cudaMemcpy(h + RN, d_dens + 7 * (size_t)RN, RN * sizeof(double), cudaMemcpyDeviceToHost);
+        double n = 0.0;
+        for (int i = 0; i < RN; i++) n += h[i];
+        for (int i = 0; i < RN; i++) n += h[RN + i];
+        free(h);
+        n *= REF_VOLEL;
+        const double req = qf_par[3] < 1.0 ? 1.0 : qf_par[3];
+        return (n - qf_par[3]) / req;
+    };
     /* initial measurement (pca.c:939-958) */
     CK(normalize_wf(nwf, d_wf, nthreads));
     CK(compute_derivatives(2 * nwf, d_wf, d_dx, d_dy, d_dz, d_lap, nthreads));
@@ -276,14 +334,16 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
     for (int im = 0; im < nmeas; im++) {
         for (int is = 0; is < nsteps; is++) {
             /* predictor (pca.c:1407-1465) */
+            qfsw = hr_switch(t0 + (it + 1) * dt, eF_run);
             CK(abm_step1(nwf, d_wf, d_f[0], d_f[1], d_f[2], d_f[3], d_f[4], INTEGRATION_SCHEME, nthreads));
             CK(normalize_wf(nwf, d_wf, nthreads));
 #ifdef FAST_CONST_EFFECTIVE_MASS_MODE
-            grads = 0;
+            grads = qfsw > 0.0 ? 1 : 0;
 #endif
             if (grads) CK(compute_derivatives(2 * nwf, d_wf, d_dx, d_dy, d_dz, d_lap, nthreads));
             else CK(compute_laplace(2 * nwf, d_wf, d_lap, nthreads));
             CK(DENS(grads));
+            if (qfsw > 0.0) CK(QFDENS());
             if (grads) CK(density_caculate_tau(d_dens, nthreads));
             CK(compute_potentials(it + 1, d_dens, d_pots, 1.0, nthreads));
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
@@ -291,16 +351,18 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
             CK(multiply_wf_by_alpha(nwf, d_wf, d_alap, d_pots, nthreads));
             CK(compute_laplace(2 * nwf, d_alap, d_alap, nthreads));
 #endif
+            if (qfsw > 0.0) pcc = host_pccoeff();
             CK(HAPPLY(it + 1, d_lap));
             /* corrector (pca.c:1469-1566) */
             CK(abm_step4(nwf, d_lap, d_wf, d_f[nh - 1], INTEGRATION_SCHEME, nthreads));
             CK(normalize_wf(nwf, d_wf, nthreads));
 #ifdef FAST_CONST_EFFECTIVE_MASS_MODE
-            grads = (is == nsteps - 1) ? 1 : 0;
+            grads = (is == nsteps - 1 || qfsw > 0.0) ? 1 : 0;
 #endif
             if (grads) CK(compute_derivatives(2 * nwf, d_wf, d_dx, d_dy, d_dz, d_lap, nthreads));
             else CK(compute_laplace(2 * nwf, d_wf, d_lap, nthreads));
             CK(DENS(grads));
+            if (qfsw > 0.0) CK(QFDENS());
             if (grads) CK(density_caculate_tau(d_dens, nthreads));
             CK(compute_potentials(it + 1, d_dens, d_pots, 1.0, nthreads));
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
@@ -311,6 +373,7 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
             Z *tmp = d_f[nh - 1];
             for (int h = nh - 1; h > 0; h--) d_f[h] = d_f[h - 1];
             d_f[0] = tmp;
+            if (qfsw > 0.0) pcc = host_pccoeff();
             CK(HAPPLY(it + 1, d_f[0]));
             it++;
         }

@@ -63,6 +63,10 @@ static int last_gradients = 0;
  * (the reference's MPI_Allreduce of the densities, pca.c:948, 1433, 1505) */
 typedef int (*exchange_fn)(void *user, double *dens, size_t count);
 static exchange_fn xfn = nullptr;
+/* quantum friction (input qfalpha, qfbeta, qfgamma, qfNreq and the qfstart/qfstop/qfswitch
+ * times in units of 1/eF) and its value in the current step */
+static double qf_alpha = 0.0, qf_beta = 0.0, qf_gamma = 0.0, qf_Nreq = 0.0, qf_start = 0.0, qf_stop = 0.0, qf_ramp = 0.0;
+static double qfsw = 0.0, pccoeff = 0.0;
 static void *xuser = nullptr;
 static void exchange_densities()
 {
@@ -389,6 +393,68 @@ static void calculate_densities(std::vector<Complex> &w, int grads)
     }
 }
 
+/* calculate_quantum_friction_densities (pca_dens.cu:365-461; cpca_dens.cu:385-450, ccpca with
+ * |k_perp|^2 and the degeneracy weight): U_a = sum f Im[u* lap u], U_b = -sum (1-f) Im[v* lap v],
+ * D = -1/2 sum (1-2f) [v* lap u + (lap v)* u], lap including -|k_perp|^2, divided by L_perp;
+ * stored after the 12 N densities as [U_a, U_b, D (complex)] */
+static void calculate_qf_densities(std::vector<Complex> &w)
+{
+    double *Ua = dens.data() + 12 * (size_t)N, *Ub = Ua + N;
+    Complex *Dq = (Complex *)(Ua + 2 * (size_t)N);
+#pragma omp parallel for
+    for (int i = 0; i < N; i++) {
+        double ua = 0.0, ub = 0.0;
+        Complex d(0.0, 0.0);
+        for (int n = 0; n < S; n++) {
+            double f = fb[n], fm = 1.0 - f, wcnt = 1.0, kp2 = 0.0;
+#if CODEDIM == 2
+            kp2 = kkz[n] * kkz[n];
+            wcnt = (std::fabs(kkz[n]) < 1.0e-12) ? 1.0 : 2.0;
+#elif CODEDIM == 1
+            kp2 = kkz[n] * kkz[n] + kky[n] * kky[n];
+            wcnt = (double)cnt[n];
+#endif
+            Complex u = U(w, n)[i], v = V(w, n)[i];
+            Complex lu = U(dlap, n)[i] - u * kp2, lv = V(dlap, n)[i] - v * kp2;
+            ua += (std::conj(u) * lu).imag() * f * wcnt;
+            ub -= (std::conj(v) * lv).imag() * fm * wcnt;
+            d += (std::conj(v) * lu + std::conj(lv) * u) * (fm - f) * wcnt;
+        }
+        const double L = WTD_LPERP;
+        Ua[i] = ua / L;
+        Ub[i] = ub / L;
+        Dq[i] = -0.5 * d / L;
+    }
+}
+
+/* the smooth switch of the friction (pca_utils.c:779-790): 0 outside (start, stop), 1 inside
+ * (start + ramp, stop - ramp), (1 + tanh(tan(pi/2 (2 s/ramp - 1))))/2 on the ramps */
+static double smooth_ramp(double s, double ramp) { return 0.5 * (1.0 + std::tanh(std::tan(M_PI_2 * (2.0 * s / ramp - 1.0)))); }
+static double smooth_step(double t, double a, double b, double ramp)
+{
+    if (t <= a || t >= b) return 0.0;
+    if (t >= a + ramp && t <= b - ramp) return 1.0;
+    if (t > a && t < a + ramp) return smooth_ramp(t - a, ramp);
+    return 1.0 - smooth_ramp(t - b + ramp, ramp);
+}
+static double qf_switch(double t)
+{
+    if (qf_alpha == 0.0 && qf_beta == 0.0 && qf_gamma == 0.0) return 0.0;
+    return smooth_step(t, qf_start / dc_eF, qf_stop / dc_eF, qf_ramp / dc_eF);
+}
+/* particle-number control coefficient (N - N_req) / N_req with N_req kept >= 1 (the reference
+ * intends this guard, pca_utils.c:1063-1072, but reads an uninitialised variable) */
+static double qf_pccoeff()
+{
+    wslda_density D = dens_view(dens.data());
+    double n = 0.0;
+    for (int i = 0; i < N; i++) n += D.rho_a[i];
+    for (int i = 0; i < N; i++) n += D.rho_b[i];
+    n *= WTD_VOLEL;
+    const double req = qf_Nreq < 1.0 ? 1.0 : qf_Nreq;
+    return (n - qf_Nreq) / req;
+}
+
 /* density_caculate_tau (pca_dens.cu:275-338): tau = max(0, lap(rho)/2 - tau_tmp) */
 static void density_tau()
 {
@@ -595,9 +661,32 @@ static void alpha_laplace(std::vector<Complex> &w)
 
 /* apply_hamiltonian (pca_kernels.cu:233-495, 674-848; cpca_kernels.cu:231-490;
  * ccpca_kernels.cu:209-448): out = (H - <H>) w.  out may alias the laplacian buffer. */
+static void filter_h_fields();
 static void apply_hamiltonian(int it, std::vector<Complex> &w, Complex *out, const double *useqpe = nullptr)
 {
     wslda_potential P = pots_view(pots.data());
+    /* quantum friction added to V_a, V_b, delta for this H only (kernel_add_quantum_friction,
+     * pca_kernels.cu:497-527; restored at the end, :530-539) */
+    std::vector<double> keep_va, keep_vb;
+    std::vector<Complex> keep_d;
+    if (qfsw > 0.0) {
+        const double qa = qf_alpha * qfsw, qb = qf_beta * qfsw, qg = qf_gamma * qfsw * pccoeff;
+        const double *Ua = dens.data() + 12 * (size_t)N, *Ub = Ua + N;
+        const Complex *Dq = (const Complex *)(Ua + 2 * (size_t)N);
+        keep_va.assign(P.V_a, P.V_a + N);
+        keep_vb.assign(P.V_b, P.V_b + N);
+        keep_d.assign(P.delta, P.delta + N);
+        for (int i = 0; i < N; i++) {
+            const double phd = std::arg(P.delta[i]), phn = std::arg(Dq[i]);
+            P.V_a[i] -= Ua[i] * qa / dc_nF;
+            P.V_b[i] -= Ub[i] * qa / dc_nF;
+            const Complex d0 = P.delta[i];
+            P.delta[i] += qb * std::abs(P.delta[i]) * Complex(std::cos(phd), std::sin(phd)) * std::sin(phd - phn);
+            P.delta[i] += Complex(0.0, qg) * d0;
+        }
+    }
+    /* the high-k filters at the top of apply_hamiltonian (pca_kernels.cu:700-704, 758-762, 791-795) */
+    filter_h_fields();
 #ifdef CURRENT_CORRECTIONS
     std::vector<double> dA[2][3], lal[2];
 #endif
@@ -757,6 +846,22 @@ static void apply_hamiltonian(int it, std::vector<Complex> &w, Complex *out, con
             out[(size_t)S * N + (size_t)n * N + i] -= V(w, n)[i] * e;
         }
     }
+    if (qfsw > 0.0) {
+#if CODEDIM == 2
+        /* the 2D engine does not remove the friction terms again (cpca_kernels.cu:846 is
+         * commented out): the potentials keep the modified, filtered fields and the friction
+         * density arrays hold the saved originals (kernel_add_quantum_friction, :521-525) */
+        double *Ua = dens.data() + 12 * (size_t)N, *Ub = Ua + N;
+        Complex *Dq = (Complex *)(Ua + 2 * (size_t)N);
+        std::copy(keep_va.begin(), keep_va.end(), Ua);
+        std::copy(keep_vb.begin(), keep_vb.end(), Ub);
+        std::copy(keep_d.begin(), keep_d.end(), Dq);
+#else
+        std::copy(keep_va.begin(), keep_va.end(), P.V_a);
+        std::copy(keep_vb.begin(), keep_vb.end(), P.V_b);
+        std::copy(keep_d.begin(), keep_d.end(), P.delta);
+#endif
+    }
 }
 
 /* the fields apply_hamiltonian filters in place before building H, at every call: V_a, V_b
@@ -780,6 +885,7 @@ static void half_step_densities(int it_next, int grads)
 {
     derivatives(y, grads);
     calculate_densities(y, grads);
+    if (qfsw > 0.0) calculate_qf_densities(y); /* pca.c:1426-1430 */
     exchange_densities();
     if (grads) density_tau();
     compute_potentials(it_next);
@@ -790,8 +896,8 @@ static void half_step_densities(int it_next, int grads)
         high_k_filter(P.alpha_b);
     }
 #endif
-    filter_h_fields();
     alpha_laplace(y);
+    if (qfsw > 0.0) pccoeff = qf_pccoeff(); /* pca.c:1458 */
 }
 
 static int scheme_slots() { return NHIST; }
@@ -854,7 +960,7 @@ int orc_setup(int nwf, const double *yin, const double *potsin, const double *fb
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
     dalap.assign(M, Complex(0, 0));
 #endif
-    dens.assign((size_t)12 * N, 0.0);
+    dens.assign((size_t)16 * N, 0.0); /* 12 N densities + 4 N quantum-friction densities */
     pots.assign(potsin, potsin + (size_t)12 * N);
     fb.assign(fbeta, fbeta + S);
     kky.assign(S, 0.0); kkz.assign(S, 0.0); cnt.assign(S, 1);
@@ -887,16 +993,17 @@ int orc_steps(int nsteps)
     for (int s = 0; s < nsteps; s++) {
         int last = (s == nsteps - 1);
         int it = it_global;
+        qfsw = qf_switch(dc_t0 + (it + 1) * dc_dt); /* pca.c:1405, 1467 */
         /* predictor */
         abm_step1(y.data(), f[0], f[1], f[2], f[3], f[4]);
         normalize(y);
-        int grads = orc_const_mass() ? 0 : 1;
+        int grads = orc_const_mass() ? (qfsw > 0.0 ? 1 : 0) : 1;
         half_step_densities(it + 1, grads);
         apply_hamiltonian(it + 1, y, dlap.data());
         /* corrector */
         abm_step4(dlap.data(), y.data(), f[NHIST - 1]);
         normalize(y);
-        grads = orc_const_mass() ? (last ? 1 : 0) : 1;
+        grads = orc_const_mass() ? ((last || qfsw > 0.0) ? 1 : 0) : 1;
         half_step_densities(it + 1, grads);
         last_gradients = grads;
         Complex *tmp = f[NHIST - 1];
@@ -905,6 +1012,7 @@ int orc_steps(int nsteps)
         apply_hamiltonian(it + 1, y, f[0]);
         it_global++;
     }
+    qfsw = 0.0; /* friction acts inside steps only */
     /* keep the rotated order visible to getters */
     std::vector<std::vector<Complex>> nv(5);
     for (int h = 0; h < NHIST; h++) nv[h].assign(f[h], f[h] + (size_t)2 * S * N);
@@ -962,7 +1070,6 @@ static void selfstart()
         alpha_laplace(y);
         /* H psi of the start state, recorded as the newest history entry */
         f3 = y;
-        filter_h_fields();
         apply_hamiltonian(0, f3, f1.data());
         qs = qpe;
         for (int h = q - 1; h > 0; h--) rec[h] = rec[h - 1];
@@ -972,7 +1079,6 @@ static void selfstart()
         for (int m = 1; m < iters; m++) {
             derivatives(f2, grads);
             alpha_laplace(f2);
-            filter_h_fields();
             apply_hamiltonian(0, f2, f1.data(), qs.data());
             taylor_term(m + 1, 0.5 * md.dt, f1, f3, f2);
         }
@@ -993,14 +1099,12 @@ static void selfstart()
         /* full step from the start state with the midpoint H */
         derivatives(y, grads);
         alpha_laplace(y);
-        filter_h_fields();
         apply_hamiltonian(0, y, f1.data());
         qs = qpe;
         taylor_term(1, md.dt, f1, y, f2);
         for (int m = 1; m < iters; m++) {
             derivatives(f2, grads);
             alpha_laplace(f2);
-            filter_h_fields();
             apply_hamiltonian(0, f2, f1.data(), qs.data());
             taylor_term(m + 1, md.dt, f1, y, f2);
         }
@@ -1089,7 +1193,7 @@ int orc_energy(double *E)
 }
 
 int orc_get_states(double *out) { std::memcpy(out, y.data(), y.size() * sizeof(Complex)); return 0; }
-int orc_get_densities(double *out) { std::memcpy(out, dens.data(), dens.size() * sizeof(double)); return 0; }
+int orc_get_densities(double *out) { std::memcpy(out, dens.data(), (size_t)12 * N * sizeof(double)); return 0; }
 int orc_get_potentials(double *out) { std::memcpy(out, pots.data(), pots.size() * sizeof(double)); return 0; }
 int orc_get_qpe(double *out) { std::memcpy(out, qpe.data(), qpe.size() * sizeof(double)); return 0; }
 int orc_get_history(int slot, double *out)
@@ -1099,6 +1203,20 @@ int orc_get_history(int slot, double *out)
     return 0;
 }
 int orc_get_it(void) { return it_global; }
+/* the quantum-friction densities of the current states (4 N: U_a, U_b, D complex) */
+int orc_qf_densities(double *out)
+{
+    derivatives(y, 0);
+    calculate_qf_densities(y);
+    std::memcpy(out, dens.data() + 12 * (size_t)N, (size_t)4 * N * sizeof(double));
+    return 0;
+}
+int orc_set_quantum_friction(double alpha, double beta, double gamma, double nreq, double start, double stop, double ramp)
+{
+    qf_alpha = alpha; qf_beta = beta; qf_gamma = gamma; qf_Nreq = nreq;
+    qf_start = start; qf_stop = stop; qf_ramp = ramp;
+    return 0;
+}
 int orc_selfstart(void)
 {
     selfstart();

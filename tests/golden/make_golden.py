@@ -63,6 +63,17 @@ SS_CASES = {
 }
 
 
+# quantum friction (pca.c:1405-1430, 1458) switched on over the run: input qfalpha, qfbeta,
+# qfgamma, qfNreq and qfstart, qfstop, qfswitch (in 1/eF)
+QF_CASES = {
+    "t2d_slda": (24, 3, 2, True),
+    "t1d_aslda": (24, 3, 2, True),
+    "c4_bdg2d": (16, 4, 1, False),
+    "t3d_aslda": (24, 3, 2, True),
+}
+QF_PARAMS = (0.5, 0.3, 0.2, 10.0, 0.0, 100.0, 0.02)
+
+
 def hkf_params(proj, mode=1):
     emax = 0.5 * np.pi ** 2 / proj.dx ** 2
     return mode, HKF_FRACTIONS[0] * emax, HKF_FRACTIONS[1] * emax
@@ -122,8 +133,9 @@ def slim(rec, n):
     return rec
 
 
-def run_case(name, out_dir, hkf=0, selfstart=False):
-    nwf, nsteps, nmeas, full = (SS_CASES if selfstart else {0: CASES, 1: HKF_CASES, 2: HKF2_CASES}[hkf])[name]
+def run_case(name, out_dir, hkf=0, selfstart=False, qf=False):
+    table = QF_CASES if qf else SS_CASES if selfstart else {0: CASES, 1: HKF_CASES, 2: HKF2_CASES}[hkf]
+    nwf, nsteps, nmeas, full = table[name]
     proj, y0, occ, pots, params, extra = case_inputs(name, nwf)
     so = os.path.join(REPO, "oracle", "_ref", name, "libref.so")
     lib = ctypes.CDLL(so, mode=ctypes.RTLD_LOCAL)
@@ -132,6 +144,8 @@ def run_case(name, out_dir, hkf=0, selfstart=False):
     lib.refh_set_hkf(mode, mu, T)
     lib.refh_set_selfstart.argtypes = [ctypes.c_int]
     lib.refh_set_selfstart(1 if selfstart else 0)
+    lib.refh_set_quantum_friction.argtypes = [ctypes.c_double] * 7
+    lib.refh_set_quantum_friction(*(QF_PARAMS if qf else (0.0,) * 7))
     lib.refh_numel.restype = ctypes.c_int
     lib.refh_nhist.restype = ctypes.c_int
     n = lib.refh_numel()
@@ -164,7 +178,7 @@ def run_case(name, out_dir, hkf=0, selfstart=False):
     if hkf:
         rec["hkf"] = np.array([mode, mu, T])
     rec = slim(rec, n)
-    path = os.path.join(out_dir, f"{name}{'_ss' if selfstart else fixture_suffix(hkf)}.npz")
+    path = os.path.join(out_dir, f"{name}{'_qf' if qf else '_ss' if selfstart else fixture_suffix(hkf)}.npz")
     np.savez_compressed(path, **rec)
     print(f"{name}: nwf={nwf} steps={nsteps}x{nmeas} E={en[:7].sum():.12g} N={en[7]:.12g},{en[8]:.12g} "
           f"ms/step={ms[0]:.3f} -> {path}")
@@ -177,6 +191,7 @@ def main():
     ap.add_argument("--hkf", type=int, default=0, choices=[0, 1, 2],
                     help="1: the effective-mass filter cases (HKF_CASES); 2: masses and pairing field (HKF2_CASES)")
     ap.add_argument("--selfstart", action="store_true", help="the Taylor self-start cases (SS_CASES)")
+    ap.add_argument("--qf", action="store_true", help="the quantum-friction cases (QF_CASES)")
     ap.add_argument("projects", nargs="*")
     a = ap.parse_args()
     if a.slim_existing:
@@ -189,9 +204,9 @@ def main():
                     np.savez_compressed(path, **slim(rec, n))
         return
     os.makedirs(a.out, exist_ok=True)
-    table = SS_CASES if a.selfstart else {0: CASES, 1: HKF_CASES, 2: HKF2_CASES}[a.hkf]
+    table = QF_CASES if a.qf else SS_CASES if a.selfstart else {0: CASES, 1: HKF_CASES, 2: HKF2_CASES}[a.hkf]
     for name in (a.projects or list(table)):
-        run_case(name, a.out, hkf=a.hkf, selfstart=a.selfstart)
+        run_case(name, a.out, hkf=a.hkf, selfstart=a.selfstart, qf=a.qf)
 
 
 if __name__ == "__main__":

@@ -59,10 +59,13 @@ class Oracle:
         L.orc_set_density_exchange.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.orc_set_high_k_filter.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
         L.orc_selfstart.restype = ctypes.c_int
+        L.orc_set_quantum_friction.argtypes = [ctypes.c_double] * 7
+        L.orc_qf_densities.argtypes = [_dp]
         L.orc_filter_field.argtypes = [_dp]
         self._xfn = None
         # the library is shared by every instance in the process: start from a plain run
         L.orc_set_high_k_filter(0, 0.0, 1.0)
+        L.orc_set_quantum_friction(0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0)
         L.orc_set_density_exchange(None, None)
         if threads:
             L.orc_set_threads(int(threads))
@@ -89,6 +92,16 @@ class Oracle:
 
     def selfstart(self):
         return self.lib.orc_selfstart()
+
+    def qf_densities(self):
+        a = np.zeros(4 * self.N)
+        self.lib.orc_qf_densities(_p(a))
+        return a
+
+    def set_quantum_friction(self, alpha, beta, gamma, nreq, start, stop, ramp):
+        """friction coefficients and the switch times (units of 1/eF), as the reference's input
+        qfalpha, qfbeta, qfgamma, qfNreq, qfstart, qfstop, qfswitch"""
+        self.lib.orc_set_quantum_friction(alpha, beta, gamma, nreq, start, stop, ramp)
 
     def set_high_k_filter(self, mode, mu, T):
         self.lib.orc_set_high_k_filter(int(mode), float(mu), float(T))

@@ -17,12 +17,14 @@ def inputs(name, nwf, seed_salt=0):
     return proj, dict(states=y0, pots=pots, occ=occ, params=params, extra=extra)
 
 
-def run_oracle(name, nwf, nsteps, nmeas=1, inp=None, threads=None, hkf=None, selfstart=False):
+def run_oracle(name, nwf, nsteps, nmeas=1, inp=None, threads=None, hkf=None, selfstart=False, qf=None):
     from oracle_lib import Oracle
     proj, d = inputs(name, nwf) if inp is None else (P.Project(name), inp)
     o = Oracle(name, threads=threads)
     if hkf is not None:
         o.set_high_k_filter(*hkf)
+    if qf is not None:
+        o.set_quantum_friction(*qf)
     o.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
     o.initial_measurement()
     if selfstart:
@@ -33,12 +35,14 @@ def run_oracle(name, nwf, nsteps, nmeas=1, inp=None, threads=None, hkf=None, sel
                 qpe=o.qpe(), history=[o.history(s) for s in range(proj.nhist)])
 
 
-def run_gpu(name, nwf, nsteps, nmeas=1, precision=0, inp=None, hkf=None, selfstart=False):
+def run_gpu(name, nwf, nsteps, nmeas=1, precision=0, inp=None, hkf=None, selfstart=False, qf=None):
     from wslda_b200 import TDRun
     proj, d = inputs(name, nwf) if inp is None else (P.Project(name), inp)
     r = TDRun(name, nwf, precision=precision)
     if hkf is not None:
         r.set_high_k_filter(*hkf)
+    if qf is not None:
+        r.set_quantum_friction(*qf)
     r.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
     r.initial_measurement()
     if selfstart:

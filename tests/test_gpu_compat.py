@@ -222,3 +222,40 @@ def test_compat_high_k_filters(has_gpu, name):
     o.set_high_k_filter(0, 0.0, 1.0)
     for x in (src, dst, zs, zd):
         x.free()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["t1d_aslda", "t2d_slda", "t3d_aslda", "c4_bdg2d"])
+def test_compat_quantum_friction_densities(has_gpu, name):
+    """calculate_quantum_friction_densities (pca_dens.cu:431 and the 2D/1D forms) against the
+    oracle on the normalised initial states"""
+    from oracle_lib import Oracle
+    from wslda_b200 import load_library
+    proj, d = inputs(name, 16)
+    N, S = proj.numel, 16
+    o = Oracle(name)
+    o.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+    o.initial_measurement()
+    want = o.qf_densities()
+    y = o.states()
+    lib = load_library(name)
+    for fn in ("gpu_malloc", "gpu_free", "memcopy_host2gpu", "memcopy_gpu2host", "create_cufftPlans"):
+        getattr(lib, fn).restype = ctypes.c_int
+    wf, lap, fb, qf = Dev(lib, y.nbytes), Dev(lib, y.nbytes), Dev(lib, S * 8), Dev(lib, 4 * N * 8)
+    wf.put(y)
+    fb.put(np.ascontiguousarray(d["occ"], dtype=np.float64))
+    assert lib.compute_laplace(2 * S, wf.p, lap.p, 512) == 0
+    if proj.codedim == 3:
+        rc = lib.calculate_quantum_friction_densities(S, wf.p, lap.p, fb.p, None, qf.p, 512)
+    elif proj.codedim == 2:
+        kk = Dev(lib, S * 8)
+        kk.put(np.zeros(S))
+        rc = lib.calculate_quantum_friction_densities(S, wf.p, lap.p, kk.p, fb.p, None, qf.p, 512)
+    else:
+        kk, cnt = Dev(lib, 2 * S * 8), Dev(lib, S * 4)
+        kk.put(np.zeros(2 * S))
+        cnt.put(np.ones(S, dtype=np.int32))
+        rc = lib.calculate_quantum_friction_densities(S, wf.p, lap.p, kk.p, fb.p, None, cnt.p, qf.p, 512)
+    assert rc == 0
+    got = qf.get(np.float64, 4 * N)
+    assert rel(got, want) < 1e-12, rel(got, want)

@@ -103,3 +103,23 @@ def test_selfstart(has_gpu, name, nwf, nsteps, nmeas):
     assert rel(g["potentials"], o["potentials"]) < TOL
     assert rel(g["states"], o["states"]) < TOL
     assert rel(g["history0"], o["history"][0]) < TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,nwf,nsteps,nmeas", [("t2d_slda", 24, 3, 2), ("t1d_aslda", 24, 3, 2), ("c4_bdg2d", 16, 4, 1),
+                                                   ("t3d_aslda", 24, 3, 2), ("t2d_vext", 24, 3, 1)])
+def test_quantum_friction(has_gpu, name, nwf, nsteps, nmeas):
+    """steps with quantum friction switched on over the run (ramp included): friction
+    densities, particle control and the friction-modified H (pca_kernels.cu:497-539)"""
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from golden.make_golden import QF_PARAMS
+    o = run_oracle(name, nwf, nsteps, nmeas, qf=QF_PARAMS)
+    g = run_gpu(name, nwf, nsteps, nmeas, qf=QF_PARAMS)
+    n = o["densities"].size // 12
+    for k, v in density_errors(g["densities"], o["densities"], n).items():
+        assert v < TOL, f"{name} density {k}: rel err {v:.3e}"
+    assert rel(g["potentials"], o["potentials"]) < TOL
+    assert rel(g["states"], o["states"]) < TOL
+    assert rel(g["qpe"], o["qpe"]) < TOL
+    assert rel(g["history0"], o["history"][0]) < TOL

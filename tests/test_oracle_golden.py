@@ -8,7 +8,7 @@ import pytest
 
 from parity_util import density_errors, inputs, rel, run_oracle
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
-from golden.make_golden import CASES, HKF2_CASES, HKF_CASES, SS_CASES, state_moments  # noqa: E402
+from golden.make_golden import CASES, HKF2_CASES, HKF_CASES, QF_CASES, QF_PARAMS, SS_CASES, state_moments  # noqa: E402
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 TOL = 1e-10
@@ -19,7 +19,8 @@ def _cases():
     hkf = [f"{n}_hkf" for n in HKF_CASES if os.path.exists(os.path.join(GOLDEN, f"{n}_hkf.npz"))]
     hkf2 = [f"{n}_hkf2" for n in HKF2_CASES if os.path.exists(os.path.join(GOLDEN, f"{n}_hkf2.npz"))]
     ss = [f"{n}_ss" for n in SS_CASES if os.path.exists(os.path.join(GOLDEN, f"{n}_ss.npz"))]
-    return plain + hkf + hkf2 + ss
+    qf = [f"{n}_qf" for n in QF_CASES if os.path.exists(os.path.join(GOLDEN, f"{n}_qf.npz"))]
+    return plain + hkf + hkf2 + ss + qf
 
 
 @pytest.mark.parametrize("name", _cases())
@@ -27,13 +28,14 @@ def test_oracle_matches_reference_golden(name):
     g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
     hkf = tuple(g["hkf"]) if "hkf" in g.files else None
     selfstart = name.endswith("_ss")
-    name = name[:-3] if selfstart else name.rsplit("_hkf", 1)[0]
+    qf = QF_PARAMS if name.endswith("_qf") else None
+    name = name[:-3] if (selfstart or qf) else name.rsplit("_hkf", 1)[0]
     nwf, nsteps, nmeas = int(g["nwf"]), int(g["nsteps"]), int(g["nmeas"])
     proj, d = inputs(name, nwf)
     # the regenerated inputs are the ones the fixture was made from
     assert rel(state_moments(d["states"], nwf, proj.numel), g["input_moments"]) < 1e-12
     o = run_oracle(name, nwf, nsteps, nmeas, inp=d, hkf=None if hkf is None else (int(hkf[0]), hkf[1], hkf[2]),
-                   selfstart=selfstart)
+                   selfstart=selfstart, qf=qf)
     if "points" in g.files:  # large lattice: fixture keeps a fixed sample of points
         idx = g["points"]
         o["densities"] = o["densities"].reshape(12, -1)[:, idx].reshape(-1)

@@ -55,6 +55,7 @@ SIGNATURES = {
     "wtd_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp]),
     "wtd_adjoint_release": (ctypes.c_int, [ctypes.c_void_p]),
     "wtd_set_high_k_filter": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double]),
+    "wtd_set_quantum_friction": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_double] * 7),
     "wtd_nccl_unique_id": (ctypes.c_int, [ctypes.c_void_p]),
     "wtd_nccl_attach": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "wtd_set_density_exchange": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
@@ -234,6 +235,12 @@ class TDRun:
         """Fermi-Dirac filter of alpha_a, alpha_b after each functional evaluation (variable
         mass); mu, T are energies"""
         self._check(self.lib.wtd_set_high_k_filter(self.h, int(mode), float(mu), float(T)))
+
+    def set_quantum_friction(self, alpha, beta, gamma, nreq, start, stop, ramp):
+        """quantum friction as the reference's input qfalpha, qfbeta, qfgamma, qfNreq, qfstart,
+        qfstop, qfswitch (times in 1/eF); all coefficients 0 turns it off"""
+        self._check(self.lib.wtd_set_quantum_friction(self.h, *[float(x) for x in (alpha, beta, gamma, nreq, start,
+                                                                                   stop, ramp)]))
 
     def adjoint_release(self):
         """free the adjoint's device workspace (kept between gradient calls)"""

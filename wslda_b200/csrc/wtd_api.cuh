@@ -53,6 +53,12 @@ struct wtd_ctx {
     /* high-k filter of the effective masses after every functional evaluation (variable mass) */
     int hkf_mode;
     double hkf_mu, hkf_T;
+    /* quantum friction: alpha, beta, gamma, N_req, start, stop, ramp (times in 1/eF); the switch
+     * value of the current step; particle-control coefficient (device); the fields H uses */
+    double qf[7];
+    double qfsw;
+    double *dqf, *qfld;
+    int sstride;                /* density-slot words per CTA: 12 N, 16 N with quantum friction */
 };
 
 static void adj_release(wtd_ctx *c);
@@ -164,6 +170,8 @@ static StepArgs make_args(wtd_ctx *c)
     a.fk_given = c->fk_given;
     a.prefetch = c->prefetch;
     a.accumulate = 0;
+    a.sstride = c->sstride;
+    a.qf = c->qfsw > 0.0 ? 1 : 0;
     return a;
 }
 
@@ -220,16 +228,18 @@ static int filter_alpha(wtd_ctx *c)
     return filter_real(c, c->pots + 4 * (size_t)WTD_NUMEL, 2);
 }
 
-static int filter_h(wtd_ctx *c)
+/* fld: [V_a, V_b, delta] to filter (the potentials, or the friction-modified copy) */
+static int filter_h(wtd_ctx *c, double *fld = NULL)
 {
     if (c->hkf_mode < 1) return WTD_OK;
     constexpr size_t N = WTD_NUMEL;
-    WTD_TRY(filter_real(c, c->pots, 2));
+    if (!fld) fld = c->pots;
+    WTD_TRY(filter_real(c, fld, 2));
 #if defined(CURRENT_CORRECTIONS) && !defined(BDG_MODE)
     WTD_TRY(filter_real(c, c->pots + 6 * N, 6));
 #endif
     if (c->hkf_mode >= 2) {
-        double2 *delta = (double2 *)(c->pots + 2 * N);
+        double2 *delta = (double2 *)(fld + 2 * N);
         if (WTD_BIG) return big_derivs(delta, 1, delta, NULL, NULL, NULL, c->tw, c->ktab, c->st, 1, c->hkf_mu, c->hkf_T);
         constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
         if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
@@ -249,10 +259,15 @@ static int filter_fields(wtd_ctx *c)
 
 /* per-point H coefficients from the potentials at time index it (variable mass: lap alpha /4
  * and -div A /2 by spectral derivatives) */
-static int coef_from_pots(wtd_ctx *c, int it)
+static int coef_from_pots(wtd_ctx *c, int it, const double *fld = NULL)
 {
     constexpr int N = WTD_NUMEL;
     wslda_potential P = convert_into_wslda_potential(c->pots, N, NULL);
+    if (fld) { /* V_a, V_b, delta from the friction-modified fields */
+        P.V_a = (double *)fld;
+        P.V_b = (double *)fld + N;
+        P.delta = (Complex *)(fld + 2 * (size_t)N);
+    }
     wtd_prep_coef<<<(N + 127) / 128, 128, 0, c->st>>>(it, P, c->cf);
     WTD_LAUNCHED(c);
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
@@ -291,10 +306,12 @@ static int functional(wtd_ctx *c, int it)
 static int after_pass(wtd_ctx *c, bool full, int it)
 {
     constexpr int N = WTD_NUMEL;
-    int nb = (12 * N + 255) / 256;
-    wtd_dens_reduce<<<nb, 256, 0, c->st>>>(c->dslot, c->grid, c->dens, N, full ? 1 : 0, 1.0 / WTD_LPERP);
+    const bool qf = c->qfsw > 0.0;
+    const int words = (qf ? 16 : 12) * N;
+    wtd_dens_reduce<<<(words + 255) / 256, 256, 0, c->st>>>(c->dslot, c->grid, c->dens, N, full ? 1 : 0, 1.0 / WTD_LPERP,
+                                                            (size_t)c->sstride, words);
     WTD_LAUNCHED(c);
-    WTD_TRY(exchange(c, c->dens, 12 * (size_t)N));
+    WTD_TRY(exchange(c, c->dens, (size_t)words));
     if (full) {
         constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
         if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
@@ -305,8 +322,42 @@ static int after_pass(wtd_ctx *c, bool full, int it)
     }
     if (it < 0) return WTD_OK;
     WTD_TRY(functional(c, it));
-    WTD_TRY(filter_fields(c));
-    return coef_from_pots(c, it);
+    WTD_TRY(filter_alpha(c));
+    if (!qf) {
+        WTD_TRY(filter_h(c));
+        return coef_from_pots(c, it);
+    }
+    /* quantum friction: H is built from V, delta plus the friction terms, filtered, while the
+     * potentials keep their values (the reference adds and removes the terms around H,
+     * pca_kernels.cu:497-539) */
+    wtd_qf_pccoeff<<<1, 512, 0, c->st>>>(c->dens, N, WTD_VOLEL, c->qf[3], c->dqf);
+    WTD_LAUNCHED(c);
+    wtd_qf_fields<<<(N + 255) / 256, 256, 0, c->st>>>(c->pots, c->dens + 12 * (size_t)N, c->dqf, c->qf[0] * c->qfsw,
+                                                      c->qf[1] * c->qfsw, c->qf[2] * c->qfsw, hc_nF, c->qfld, N);
+    WTD_LAUNCHED(c);
+    WTD_TRY(filter_h(c, c->qfld));
+    WTD_TRY(coef_from_pots(c, it, c->qfld));
+#if CODEDIM == 2
+    /* the 2D engine leaves the friction terms in (cpca_kernels.cu:846 commented out): the
+     * potentials take the modified, filtered fields and the friction-density words the
+     * originals (kernel_add_quantum_friction, cpca_kernels.cu:521-525) */
+    WTD_CU(cudaMemcpyAsync(c->dens + 12 * (size_t)N, c->pots, 4 * (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    WTD_CU(cudaMemcpyAsync(c->pots, c->qfld, 4 * (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+#endif
+    return WTD_OK;
+}
+
+/* the friction switch at time t (pca_utils.c:779-790, 1055-1060): 0 when every coefficient is
+ * 0, else the smooth step of the qfstart/qfstop/qfswitch times (1/eF) */
+static double qf_switch(const wtd_ctx *c, double t)
+{
+    if (c->qf[0] == 0.0 && c->qf[1] == 0.0 && c->qf[2] == 0.0) return 0.0;
+    const double a = c->qf[4] / hc_eF, b = c->qf[5] / hc_eF, r = c->qf[6] / hc_eF;
+    auto ramp = [](double x, double T) { return 0.5 * (1.0 + tanh(tan(M_PI_2 * (2.0 * x / T - 1.0)))); };
+    if (t <= a || t >= b) return 0.0;
+    if (t >= a + r && t <= b - r) return 1.0;
+    if (t > a && t < a + r) return ramp(t - a, r);
+    return 1.0 - ramp(t - b + r, r);
 }
 
 /* ---------------------------------------------------------------------------------------
@@ -436,13 +487,16 @@ static int fused_step(wtd_ctx *c, bool last, StepRecord *rec, double2 *yk_next =
     const bool var = WTD_VAR;
     constexpr int N = WTD_NUMEL;
     if (!c->fk_given && !c->have_coef) return WTD_ERR_STATE;
+    /* quantum friction of this step (pca.c:1405, 1467): gradients and friction densities */
+    c->qfsw = qf_switch(c, hc_t0 + (c->it + 1) * c->dt);
+    const bool qf = c->qfsw > 0.0;
     if (rec) {
         WTD_CU(cudaMemcpyAsync(rec->cfA, c->cf, CF_COUNT * (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
         rec->hasH = c->fk_given ? 0 : 1;
     }
     /* predictor: f_k, y_pred, P; densities of y_pred */
     if (!rec) {
-        WTD_TRY(run_pass(c, 0, var));
+        WTD_TRY(run_pass(c, 0, var || qf));
     } else {
         StepArgs a = make_args(c);
         a.y = rec->yk;
@@ -451,10 +505,10 @@ static int fused_step(wtd_ctx *c, bool last, StepRecord *rec, double2 *yk_next =
         a.qpe = rec->EA;
         WTD_TRY((var ? launch_pass<0, true>(c, a) : launch_pass<0, false>(c, a)));
     }
-    WTD_TRY(after_pass(c, var, c->it + 1));
+    WTD_TRY(after_pass(c, var || qf, c->it + 1));
     if (rec) WTD_CU(cudaMemcpyAsync(rec->cfB, c->cf, CF_COUNT * (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
     /* corrector */
-    const bool g = var || last;
+    const bool g = var || last || qf;
     if (!rec) {
         WTD_TRY(run_pass(c, 1, g));
     } else {
@@ -523,7 +577,7 @@ size_t wtd_device_bytes(int nwf, int precision)
 {
     size_t n2 = (size_t)2 * nwf * WTD_NUMEL;
     size_t b = n2 * (elem_bytes_y(precision) + WTD_NHIST * elem_bytes_h(precision)) +
-               (size_t)300 * 12 * WTD_NUMEL * sizeof(double);
+               (size_t)300 * 16 * WTD_NUMEL * sizeof(double);
     if (WTD_BIG) b += n2 * sizeof(double2) * ((CODEDIM >= 3 ? 4 : 3) + (WTD_VAR ? 1 : 0));
     return b;
 }
@@ -583,9 +637,11 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     ALLOC(c->occ, nwf * sizeof(double));
     ALLOC(c->kp2, nwf * sizeof(double));
     ALLOC(c->wcnt, nwf * sizeof(double));
-    ALLOC(c->dslot, (size_t)c->grid * 12 * N * sizeof(double));
+    ALLOC(c->dslot, (size_t)c->grid * 16 * N * sizeof(double)); /* 12 N words, 16 N with quantum friction */
     ALLOC(c->qpe, nwf * sizeof(double));
-    ALLOC(c->dens, 12 * N * sizeof(double));
+    ALLOC(c->dens, 16 * N * sizeof(double));
+    ALLOC(c->qfld, 4 * N * sizeof(double));
+    ALLOC(c->dqf, 4 * sizeof(double));
     ALLOC(c->pots, 12 * N * sizeof(double));
     ALLOC(c->ework, (size_t)TDWSLDAITEMS * N * sizeof(double));
     ALLOC(c->eout, 16 * sizeof(double));
@@ -605,7 +661,9 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     if (e != cudaSuccess) { wtd_destroy(c); return e == cudaErrorMemoryAllocation ? WTD_ERR_NOMEM : WTD_ERR_CUDA; }
     cudaMemsetAsync(c->cf, 0, (size_t)CF_COUNT * N * sizeof(double), c->st);
     cudaMemsetAsync(c->qpe, 0, nwf * sizeof(double), c->st);
-    cudaMemsetAsync(c->dens, 0, 12 * N * sizeof(double), c->st);
+    cudaMemsetAsync(c->dens, 0, 16 * N * sizeof(double), c->st);
+    cudaMemsetAsync(c->dqf, 0, 4 * sizeof(double), c->st);
+    c->sstride = 12 * (int)N;
     {
         double2 tw[WG::twtotal];
         double kt[6 * WTD_KT];
@@ -642,7 +700,7 @@ int wtd_destroy(wtd_ctx *c)
         for (int p = 0; p < 2; p++)
             for (int k = 0; k < 2; k++)
                 for (int i = 0; i < 4096; i++) cudaEventDestroy(c->ev[p][k][i]);
-    void *ptrs[] = {c->y, c->cf, c->occ, c->kp2, c->wcnt, c->dslot, c->qpe, c->dens, c->pots, c->ework,
+    void *ptrs[] = {c->y, c->cf, c->occ, c->kp2, c->wcnt, c->dslot, c->qpe, c->dens, c->pots, c->qfld, c->dqf, c->ework,
                     c->eout, c->tw, c->ktab, c->stage, c->extra, c->ddx, c->ddy, c->ddz, c->dlap, c->dalap, c->stage3d};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) if (ptrs[i]) cudaFree(ptrs[i]);
     for (int h = 0; h < WTD_NHIST; h++) if (c->hist[h]) cudaFree(c->hist[h]);
@@ -820,6 +878,7 @@ int wtd_initial_measurement(wtd_ctx *c, int it0)
     WTD_CU(cudaSetDevice(c->dev));
     c->it = it0;
     c->head = 0;
+    c->qfsw = 0.0;
     for (int h = 0; h < WTD_NHIST; h++) WTD_CU(cudaMemsetAsync(c->hist[h], 0, c->hsz, c->st));
     c->fk_given = 1;
     if (c->staged) {
@@ -971,6 +1030,18 @@ int wtd_nccl_attach(wtd_ctx *c, const void *id128, int nranks, int rank)
     return WTD_OK;
 }
 
+int wtd_set_quantum_friction(wtd_ctx *c, double alpha, double beta, double gamma, double nreq, double start,
+                             double stop, double ramp)
+{
+    if (!c) return WTD_ERR_ARG;
+    const bool on = alpha != 0.0 || beta != 0.0 || gamma != 0.0;
+    if (on && (c->staged || !(ramp > 0.0))) return c->staged ? WTD_ERR_UNSUPPORTED : WTD_ERR_ARG;
+    c->qf[0] = alpha; c->qf[1] = beta; c->qf[2] = gamma; c->qf[3] = nreq;
+    c->qf[4] = start; c->qf[5] = stop; c->qf[6] = ramp;
+    c->sstride = (on ? 16 : 12) * WTD_NUMEL;
+    return WTD_OK;
+}
+
 int wtd_set_high_k_filter(wtd_ctx *c, int mode, double mu, double T)
 {
     if (!c || (mode >= 1 && !(T > 0.0))) return WTD_ERR_ARG;
@@ -1086,6 +1157,7 @@ static int selfstart_run(wtd_ctx *c, SelfWork &w)
     /* work arrays: the physical history slots, overwritten by the history at the end */
     double2 *f1 = (double2 *)c->hist[0], *f2 = (double2 *)c->hist[1], *f3 = (double2 *)c->hist[2];
     const double dt = c->dt;
+    c->qfsw = 0.0; /* no friction during the self-start (pca.c:1113, 1209) */
     for (int step = 0; step < q; step++) {
         /* start state: densities and potentials at time index 0, its (H - <H>) psi recorded */
         WTD_TRY(ss_derivs(c, w, y, grads));
@@ -1477,7 +1549,7 @@ extern "C" int wtd_adjoint(wtd_ctx *c, int it0, int nsteps, int checkpoint_every
         (grad && nparam < 1))
         return WTD_ERR_ARG;
 #if defined(WTD_ADJOINT_CONTACT_BDG) && defined(FAST_CONST_EFFECTIVE_MASS_MODE)
-    if (c->prec != WTD_FP64 || c->staged) return WTD_ERR_UNSUPPORTED;
+    if (c->prec != WTD_FP64 || c->staged || c->sstride != 12 * WTD_NUMEL) return WTD_ERR_UNSUPPORTED;
     WTD_CU(cudaSetDevice(c->dev));
     const int r = adjoint_run(c, it0, nsteps, checkpoint_every, mask, nparam, loss, grad);
     if (r != WTD_OK) cudaStreamSynchronize(c->st);

@@ -11,16 +11,52 @@
 /* dens[i] = sum_s slot[s][i] / L_perp over the 12N density words (fixed slot order, so the
  * result is bitwise reproducible).  Limited mode keeps nu, rho_a, rho_b and zeroes the rest,
  * as kernel_calculate_densities_limited does (pca_dens.cu:133-198). */
-__global__ void wtd_dens_reduce(const double *slots, int nslots, double *dens, int N, int full, double inv_lperp)
+__global__ void wtd_dens_reduce(const double *slots, int nslots, double *dens, int N, int full, double inv_lperp,
+                                size_t stride = 0, int words = 0)
 {
+    /* words: 12 N, or 16 N with the quantum-friction densities [U_a, U_b, D] after them;
+     * stride: slot words per CTA */
+    if (!stride) stride = 12 * (size_t)N;
+    if (!words) words = 12 * N;
     int i = threadIdx.x + blockIdx.x * blockDim.x;
-    if (i >= 12 * N) return;
+    if (i >= words) return;
     int q = (i < 2 * N) ? 0 : 1 + (i - 2 * N) / N; /* 0: nu, 1: rho_a, 2: tau_a, ..., 6: rho_b ... */
-    bool needed = full || q == 0 || q == 1 || q == 6;
+    bool needed = full || q == 0 || q == 1 || q == 6 || i >= 12 * N;
     double s = 0.0;
     if (needed)
-        for (int k = 0; k < nslots; k++) s += slots[(size_t)k * 12 * N + i];
+        for (int k = 0; k < nslots; k++) s += slots[(size_t)k * stride + i];
     dens[i] = s * inv_lperp;
+}
+
+/* the quantum-friction particle-control coefficient (N - N_req) / N_req, N = volel *
+ * sum(rho_a + rho_b), N_req kept >= 1 (pca_utils.c:1063-1072; the reference reads an
+ * uninitialised divisor there, this takes the guard it intends) -> out[0] */
+__global__ void __launch_bounds__(512) wtd_qf_pccoeff(const double *dens, int N, double volel, double nreq, double *out)
+{
+    __shared__ double red[80];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s += dens[2 * (size_t)N + i] + dens[7 * (size_t)N + i];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) out[0] = (s * volel - nreq) / (nreq < 1.0 ? 1.0 : nreq);
+}
+
+/* the fields H is built from while quantum friction acts (kernel_add_quantum_friction,
+ * pca_kernels.cu:497-527), into fld = [V_a, V_b, delta (complex)] without touching the
+ * potentials: V_s - U_s qa / nF, delta + qb |delta| e^{i phi} sin(phi - phi_D) + i qg pcc delta */
+__global__ void wtd_qf_fields(const double *pots, const double *qfd, const double *pcc, double qa, double qb, double qg,
+                              double nF, double *fld, int N)
+{
+    int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i >= N) return;
+    const double *Ua = qfd, *Ub = qfd + N;
+    const Complex *Dq = (const Complex *)(qfd + 2 * (size_t)N);
+    const Complex d0 = ((const Complex *)(pots + 2 * (size_t)N))[i];
+    fld[i] = pots[i] - Ua[i] * qa / nF;
+    fld[N + i] = pots[N + i] - Ub[i] * qa / nF;
+    const double phd = thrust::arg(d0), phn = thrust::arg(Dq[i]);
+    Complex d = d0 + qb * thrust::abs(d0) * Complex(cos(phd), sin(phd)) * sin(phd - phn);
+    d += Complex(0.0, qg * pcc[0]) * d0;
+    ((Complex *)(fld + 2 * (size_t)N))[i] = d;
 }
 
 /* ---------------------------------------------------------------------------------------

@@ -293,6 +293,36 @@ __global__ void k_overlap(int n, const double2 *a, const double2 *b, double *re,
     }
 }
 
+/* calculate_quantum_friction_densities (pca_dens.cu:365-461; cpca_dens.cu:385-450; ccpca): one
+ * thread per point, states in order; out = [U_a, U_b, D (complex)] */
+__global__ void k_qf_dens_compat(int n, const double2 *wf, const double2 *lap, const double *fb, const double *wts,
+                                 const double *kp2, const double *wcnt, double *out, double inv_lperp)
+{
+    constexpr int N = WTD_NUMEL;
+    const int p = threadIdx.x + blockIdx.x * blockDim.x;
+    if (p >= N) return;
+    const size_t SN = (size_t)n * N;
+    double ua = 0.0, ub = 0.0, dre = 0.0, dim = 0.0;
+    for (int s = 0; s < n; s++) {
+        double f = fb[s], fm = 1.0 - f;
+        if (wts) { f *= wts[s]; fm *= wts[s]; }
+        const double wc = wcnt[s], k2 = kp2[s];
+        const size_t iu = (size_t)s * N + p, iv = SN + iu;
+        const double2 u = wf[iu], v = wf[iv];
+        const double2 lu = make_double2(lap[iu].x - u.x * k2, lap[iu].y - u.y * k2);
+        const double2 lv = make_double2(lap[iv].x - v.x * k2, lap[iv].y - v.y * k2);
+        ua += (u.x * lu.y - u.y * lu.x) * f * wc;
+        ub -= (v.x * lv.y - v.y * lv.x) * fm * wc;
+        /* v* lu + lv* u */
+        dre += ((v.x * lu.x + v.y * lu.y) + (lv.x * u.x + lv.y * u.y)) * (fm - f) * wc;
+        dim += ((v.x * lu.y - v.y * lu.x) + (lv.x * u.y - lv.y * u.x)) * (fm - f) * wc;
+    }
+    out[p] = ua * inv_lperp;
+    out[N + p] = ub * inv_lperp;
+    out[2 * (size_t)N + 2 * p] = -0.5 * dre * inv_lperp;
+    out[2 * (size_t)N + 2 * p + 1] = -0.5 * dim * inv_lperp;
+}
+
 /* out += a (+ b) */
 __global__ void k_add_fields(double *out, const double *a, const double *b, int n)
 {
@@ -358,9 +388,14 @@ static int compat_real_deriv(const double *f, double *out, int which)
 }
 
 /* per-point coefficients from the potentials (+ lap alpha, div A for variable mass) */
-static int compat_coefficients(int it, double *pots)
+static int compat_coefficients(int it, double *pots, const double *fld = NULL)
 {
     wslda_potential P = convert_into_wslda_potential(pots, WTD_NUMEL, NULL);
+    if (fld) { /* V_a, V_b, delta with the friction terms */
+        P.V_a = (double *)fld;
+        P.V_b = (double *)fld + WTD_NUMEL;
+        P.delta = (Complex *)(fld + 2 * (size_t)WTD_NUMEL);
+    }
     double *cf = compat_cf();
     wtd_prep_coef<<<(WTD_NUMEL + 127) / 128, 128>>>(it, P, cf);
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
@@ -803,20 +838,37 @@ int multiply_wf_by_alpha(int n, wtd_z *in, wtd_z *out, double *pots, int nthread
     return cu_sync_status();
 }
 
+/* the friction-modified V_a, V_b, delta (4 N) and the control coefficient on the device */
+static double *g_qfld = NULL, *g_pcc = NULL;
+
 static int apply_hamiltonian_impl(int it, int n, wtd_z *in, wtd_z *out, wtd_z *dx, wtd_z *dy, wtd_z *dz, wtd_z *lap,
-                                  wtd_z *alap, const double *kky, const double *kkz, double *pots, double qfswitch, double *useqpe)
+                                  wtd_z *alap, const double *kky, const double *kkz, double *dens, double *pots,
+                                  double qfswitch, double *useqpe, double pccoeff)
 {
-    if (qfswitch > 0.0) return WTD_ERR_UNSUPPORTED;
     if (!g_work || g_nwfip < n) return WTD_ERR_STATE;
+    /* quantum friction (pca_kernels.cu:497-539): H from V, delta plus the friction terms, the
+     * potentials left as they are; the V and delta filters then act on that copy only */
+    double *fld = pots;
+    if (qfswitch > 0.0) {
+        if (!dens) return WTD_ERR_ARG;
+        if (!g_qfld) {
+            if (cudaMalloc((void **)&g_qfld, 4 * sizeof(double) * WTD_NUMEL) != cudaSuccess) return WTD_ERR_NOMEM;
+            if (cudaMalloc((void **)&g_pcc, sizeof(double)) != cudaSuccess) return WTD_ERR_NOMEM;
+        }
+        cudaMemcpy(g_pcc, &pccoeff, sizeof(double), cudaMemcpyHostToDevice);
+        wtd_qf_fields<<<(WTD_NUMEL + 255) / 256, 256>>>(pots, dens + 12 * (size_t)WTD_NUMEL, g_pcc, md.qfalpha * qfswitch,
+                                                        md.qfbeta * qfswitch, md.qfgamma * qfswitch, hc_nF, g_qfld, WTD_NUMEL);
+        fld = g_qfld;
+    }
     /* high-k filters of the fields, in place, as the reference's apply_hamiltonian: V_a, V_b
      * (hkf_mode >= 1, pca_kernels.cu:700-704), delta (>= 2, :758-762), the A components
      * (>= 1 with current corrections outside BdG, :791-795) */
     if (md.hkf_mode >= 1) {
-        int rf = high_frequency_filter_massive_d(2, pots, pots, md.hkf_mu, md.hkf_T, 512);
+        int rf = high_frequency_filter_massive_d(2, fld, fld, md.hkf_mu, md.hkf_T, 512);
         if (rf) return rf;
     }
     if (md.hkf_mode >= 2) {
-        wtd_z *delta = (wtd_z *)(pots + 2 * (size_t)WTD_NUMEL);
+        wtd_z *delta = (wtd_z *)(fld + 2 * (size_t)WTD_NUMEL);
         int rf = high_frequency_filter_c(delta, delta, md.hkf_mu, md.hkf_T, 512);
         if (rf) return rf;
     }
@@ -827,13 +879,21 @@ static int apply_hamiltonian_impl(int it, int n, wtd_z *in, wtd_z *out, wtd_z *d
         if (rf) return rf;
     }
 #endif
-    int r = compat_coefficients(it, pots);
+    int r = compat_coefficients(it, pots, fld == pots ? NULL : fld);
     if (r) return r;
     r = compat_planewave(n, kky, kkz, NULL);
     if (r) return r;
     k_hamiltonian_compat<<<n, 256>>>(n, (const double2 *)in, (double2 *)out, (const double2 *)dx, (const double2 *)dy,
                                      (const double2 *)dz, (const double2 *)lap, (const double2 *)alap, compat_cf(), g_kp2,
                                      compat_qpe(), useqpe);
+#if CODEDIM == 2
+    if (fld != pots) {
+        /* the 2D engine does not remove the friction terms (cpca_kernels.cu:846 commented out):
+         * the potentials keep the modified fields, the friction densities the originals */
+        cudaMemcpy(dens + 12 * (size_t)WTD_NUMEL, pots, 4 * sizeof(double) * WTD_NUMEL, cudaMemcpyDeviceToDevice);
+        cudaMemcpy(pots, fld, 4 * sizeof(double) * WTD_NUMEL, cudaMemcpyDeviceToDevice);
+    }
+#endif
     return cu_sync_status();
 }
 
@@ -841,19 +901,49 @@ static int apply_hamiltonian_impl(int it, int n, wtd_z *in, wtd_z *out, wtd_z *d
 int apply_hamiltonian(int it, int n, wtd_z *in, wtd_z *out, wtd_z *dx, wtd_z *dy, wtd_z *dz, wtd_z *lap, wtd_z *alap,
                       double *dens, double *pots, double qfswitch, double *useqpe, double pccoeff, int nthreads)
 {
-    return apply_hamiltonian_impl(it, n, in, out, dx, dy, dz, lap, alap, NULL, NULL, pots, qfswitch, useqpe);
+    return apply_hamiltonian_impl(it, n, in, out, dx, dy, dz, lap, alap, NULL, NULL, dens, pots, qfswitch, useqpe, pccoeff);
 }
 #elif CODEDIM == 2
 int apply_hamiltonian(int it, int n, wtd_z *in, wtd_z *out, wtd_z *dx, wtd_z *dy, double *kkz, wtd_z *lap, wtd_z *alap,
                       double *dens, double *pots, double qfswitch, double *useqpe, double pccoeff, int nthreads)
 {
-    return apply_hamiltonian_impl(it, n, in, out, dx, dy, NULL, lap, alap, NULL, kkz, pots, qfswitch, useqpe);
+    return apply_hamiltonian_impl(it, n, in, out, dx, dy, NULL, lap, alap, NULL, kkz, dens, pots, qfswitch, useqpe, pccoeff);
 }
 #else
 int apply_hamiltonian(int it, int n, wtd_z *in, wtd_z *out, wtd_z *dx, double *kkyz, wtd_z *lap, wtd_z *alap,
                       double *dens, double *pots, double qfswitch, double *useqpe, double pccoeff, int nthreads)
 {
-    return apply_hamiltonian_impl(it, n, in, out, dx, NULL, NULL, lap, alap, kkyz, kkyz ? kkyz + n : NULL, pots, qfswitch, useqpe);
+    return apply_hamiltonian_impl(it, n, in, out, dx, NULL, NULL, lap, alap, kkyz, kkyz ? kkyz + n : NULL, dens, pots, qfswitch,
+                                  useqpe, pccoeff);
+}
+#endif
+
+static int calculate_qf_densities_impl(int n, const wtd_z *wf, const wtd_z *lap, const double *kky, const double *kkz,
+                                const int *cnt, const double *fb, const double *w, double *qf)
+{
+    if (n <= 0 || !wf || !lap || !fb || !qf) return WTD_ERR_ARG;
+    int r = compat_planewave(n, kky, kkz, cnt);
+    if (r) return r;
+    k_qf_dens_compat<<<(WTD_NUMEL + 255) / 256, 256>>>(n, (const double2 *)wf, (const double2 *)lap, fb, w, g_kp2, g_wcnt,
+                                                       qf, 1.0 / WTD_LPERP);
+    return cu_sync_status();
+}
+#if CODEDIM == 3
+int calculate_quantum_friction_densities(int n, wtd_z *wf, wtd_z *lap, double *fb, double *w, double *qf, int nthreads)
+{
+    return calculate_qf_densities_impl(n, wf, lap, NULL, NULL, NULL, fb, w, qf);
+}
+#elif CODEDIM == 2
+int calculate_quantum_friction_densities(int n, wtd_z *wf, wtd_z *lap, double *kkz, double *fb, double *w, double *qf,
+                                         int nthreads)
+{
+    return calculate_qf_densities_impl(n, wf, lap, NULL, kkz, NULL, fb, w, qf);
+}
+#else
+int calculate_quantum_friction_densities(int n, wtd_z *wf, wtd_z *lap, double *kkyz, double *fb, double *w, int *cnt,
+                                         double *qf, int nthreads)
+{
+    return calculate_qf_densities_impl(n, wf, lap, kkyz, kkyz ? kkyz + n : NULL, cnt, fb, w, qf);
 }
 #endif
 

@@ -69,6 +69,8 @@ struct StepArgs {
     int fk_given;       /* pass A: f_k is already in ring slot NH-1 */
     int prefetch;       /* bit 0: next state's y, bit 1: this state's ABM history into L2 */
     int accumulate;     /* add to the density slot (otherwise start from zero) */
+    int sstride;        /* density-slot words per CTA: 12 N, or 16 N with quantum friction */
+    int qf;             /* accumulate the quantum-friction densities (needs GRAD) */
 };
 
 /* ABM coefficients (tdwslda_ode_integrator.h:44-45, 69-70, 94-95, 153, 172, 191) */
@@ -336,11 +338,16 @@ __device__ __forceinline__ void dens_limited(double *ds, int p, int N, double2 u
 template <class G, typename TY, typename TC>
 __device__ __forceinline__ void dens_gradients(double *ds, const TY *ysrc, typename cplx<TC>::t *B0,
                                                typename cplx<TC>::t *W, const typename cplx<TC>::t *tw,
-                                               const double (*kt)[WTD_KT], double f, double w, double kp2, int comp)
+                                               const double (*kt)[WTD_KT], double f, double w, double kp2, int comp,
+                                               const TY *yother = nullptr)
 {
     typedef typename cplx<TC>::t C;
     constexpr int N = G::ntot;
     const double fw = (comp == 0 ? f : (1.0 - f)) * w;
+    /* quantum-friction densities when yother (the other component) is given, after the 12 N
+     * density words (pca_dens.cu:365-461): U_a += f Im[u* lap u], U_b -= (1-f) Im[v* lap v],
+     * D += -1/2 (1-2f) [v* lap u + (lap v)* u], lap including -|k_perp|^2 */
+    const double fq = (1.0 - 2.0 * f) * w * -0.5;
     const int tau_q = comp == 0 ? 3 : 8, j_q = comp == 0 ? 4 : 9;
     const double jsgn = comp == 0 ? 1.0 : -1.0;
     __syncthreads();
@@ -361,6 +368,21 @@ __device__ __forceinline__ void dens_gradients(double *ds, const TY *ysrc, typen
             if (op == 0) {
                 double lx = dx - sv.x * kp2, ly = dy - sv.y * kp2;
                 ds[tau_q * (size_t)N + p] += (sv.x * lx + sv.y * ly) * fw;
+                if (yother) {
+                    const double2 o = to_d(yother[p]);
+                    const double im = sv.x * ly - sv.y * lx; /* Im[psi* lap psi] */
+                    if (comp == 0) {
+                        ds[12 * (size_t)N + p] += im * fw;
+                        /* v* lap u */
+                        ds[14 * (size_t)N + 2 * p] += (o.x * lx + o.y * ly) * fq;
+                        ds[14 * (size_t)N + 2 * p + 1] += (o.x * ly - o.y * lx) * fq;
+                    } else {
+                        ds[13 * (size_t)N + p] -= im * fw;
+                        /* (lap v)* u */
+                        ds[14 * (size_t)N + 2 * p] += (lx * o.x + ly * o.y) * fq;
+                        ds[14 * (size_t)N + 2 * p + 1] += (lx * o.y - ly * o.x) * fq;
+                    }
+                }
             } else {
                 ds[(j_q + op - 1) * (size_t)N + p] += jsgn * (sv.x * dy - sv.y * dx) * fw;
             }
@@ -399,9 +421,9 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
     TY *Y = (TY *)a.y;
     TY *YO = a.yout ? (TY *)a.yout : Y;
     const uint64_t pol = l2_policy_keep();
-    double *ds = a.dslot + (size_t)blockIdx.x * 12 * N;
+    double *ds = a.dslot + (size_t)blockIdx.x * a.sstride;
     if (!a.accumulate)
-        for (int i = threadIdx.x; i < 12 * N; i += blockDim.x) ds[i] = 0.0;
+        for (int i = threadIdx.x; i < a.sstride; i += blockDim.x) ds[i] = 0.0;
     const double dt = a.dt;
     const size_t SN = (size_t)a.S * N;
 
@@ -548,8 +570,8 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
             /* const mass: (HU, HV) = (BU, BV) hold the state, B2 is work.
              * variable mass: (HU, HV) = (B2, B3), BU is work. */
             C *Wk = VAR ? BU : B2;
-            dens_gradients<G, TY, TC>(ds, ou, HU, Wk, tw, kt, f, w, kp2, 0);
-            dens_gradients<G, TY, TC>(ds, ov, HV, Wk, tw, kt, f, w, kp2, 1);
+            dens_gradients<G, TY, TC>(ds, ou, HU, Wk, tw, kt, f, w, kp2, 0, a.qf ? ov : nullptr);
+            dens_gradients<G, TY, TC>(ds, ov, HV, Wk, tw, kt, f, w, kp2, 1, a.qf ? ou : nullptr);
         }
         __syncthreads();
     }
