@@ -106,6 +106,10 @@ int wtd_download_densities(wtd_ctx *ctx, double *host_dens);
 int wtd_download_potentials(wtd_ctx *ctx, double *host_pots);
 /* <psi_n|H|psi_n> dV of the last H application (left in d_workarea by the reference) */
 int wtd_download_qpe(wtd_ctx *ctx, double *host_qpe);
+/* densities (12 N, with tau and j) of a weighted subset of the current states: the reference's
+ * subset tracking (pca.c:842-870, 1056-1066) with weights[n] = 1 for the tracked states, 0
+ * otherwise (any real weights are accepted).  FP64. */
+int wtd_subset_densities(wtd_ctx *ctx, const double *weights, double *host_dens);
 
 /* device pointers (for callers that keep data on the GPU): states, densities, potentials */
 int wtd_device_pointers(wtd_ctx *ctx, void **states, double **dens, double **pots);

@@ -342,9 +342,11 @@ static void derivatives(std::vector<Complex> &w, int grads)
 }
 
 /* calculate_densities (pca_dens.cu:13-198; cpca_dens.cu:14-140; ccpca_dens.cu:14-140) */
-static void calculate_densities(std::vector<Complex> &w, int grads)
+static void calculate_densities(std::vector<Complex> &w, int grads, const double *weights = nullptr,
+                                double *into = nullptr)
 {
-    wslda_density D = dens_view(dens.data());
+    /* weights: per-state factors of the subset densities (pca_dens.cu:46-47), into: output */
+    wslda_density D = dens_view(into ? into : dens.data());
     const double DF = 10000.;
 #pragma omp parallel for
     for (int i = 0; i < N; i++) {
@@ -352,6 +354,7 @@ static void calculate_densities(std::vector<Complex> &w, int grads)
         Complex nu(0.0, 0.0);
         for (int n = 0; n < S; n++) {
             double fbEn = fb[n] * DF, fbmEn = DF - fbEn;
+            if (weights) { fbEn *= weights[n]; fbmEn *= weights[n]; }
             double wcnt = 1.0, kp2 = 0.0;
 #if CODEDIM == 2
             double kz = kkz[n];
@@ -456,9 +459,9 @@ static double qf_pccoeff()
 }
 
 /* density_caculate_tau (pca_dens.cu:275-338): tau = max(0, lap(rho)/2 - tau_tmp) */
-static void density_tau()
+static void density_tau(double *into = nullptr)
 {
-    wslda_density D = dens_view(dens.data());
+    wslda_density D = dens_view(into ? into : dens.data());
     std::vector<double> lr(N);
     double *rho[2] = {D.rho_b, D.rho_a}, *tau[2] = {D.tau_b, D.tau_a};
     for (int s = 0; s < 2; s++) {
@@ -620,6 +623,115 @@ static void potentials_point(int it, int i, wslda_density Dn, wslda_potential P,
         }
     }
 #endif
+    P.V_a[i] = Va; P.V_b[i] = Vb; P.delta[i] = ldelta;
+}
+#elif FUNCTIONAL == SLDAE
+/* tdwslda_functionals.h:530-812 */
+static void potentials_point(int it, int i, wslda_density Dn, wslda_potential P, double cccoeff)
+{
+    using namespace oedf;
+    using namespace osldae;
+    int ix, iy, iz; decode(i, ix, iy, iz);
+    double Va_const = ORC_U_EXT(ix, iy, iz, it, SPINA);
+    double Vb_const = ORC_U_EXT(ix, iy, iz, it, SPINB);
+    double na = Dn.rho_a[i], nb = Dn.rho_b[i];
+    double taua = Dn.tau_a[i], taub = Dn.tau_b[i];
+    Complex lnu = Dn.nu[i];
+    double Va = P.V_a[i], Vb = P.V_b[i];
+    Complex ldelta = P.delta[i];
+    double nt = na + nb;
+    double nt_1o3 = std::pow(nt, 1. / 3.), nt_2o3 = std::pow(nt, 2. / 3.);
+    double kF = std::pow(3. * std::pow(M_PI, 2) * nt, 1. / 3.);
+    double eF = std::pow(kF, 2) / 2.;
+    double as = scattering_length(ix, iy, iz, it, dc_params, dc_extra_data_size, dc_extra_data);
+    double x = std::fabs(as * kF);
+    double nt_reg = p_reg(nt);
+    double dx_dnt = (nt_reg > 0.0) ? nt_reg * x / (3. * nt) : 0.0;
+    double beta = beta_d0(x), inverse_gamma = inverse_gamma_d0(x);
+    double alpha_p = dx_dnt * alpha_d1(x);
+    double af = a_functional_d0(x), cf = c_functional_d0(x);
+    double af_p = 0.0, cf_p = 0.0;
+    if (nt_reg > 0.0) {
+        af_p = alpha_p;
+        cf_p = nt_reg * cf / (3. * nt) * (1. - cf * inverse_gamma);
+    }
+    double ctilde = af * nt_1o3 / cf;
+    double inverse_gamma_eff = (1 / cf) * (1. - 3. * nt / cf * cf_p);
+    double ctilde_p = (nt_reg > 0.) ? std::pow(nt_reg, 2. / 3.) * inverse_gamma_eff * af / (3. * nt_2o3) : 0.;
+    ctilde_p += af_p * nt_1o3 / cf;
+#ifdef CURRENT_CORRECTIONS
+    P.alpha_a[i] = af; P.alpha_b[i] = af;
+    double *Aa[3] = {P.A_a_x, P.A_a_y, P.A_a_z}, *Ab[3] = {P.A_b_x, P.A_b_y, P.A_b_z};
+    double *ja[3] = {Dn.j_a_x, Dn.j_a_y, Dn.j_a_z}, *jb[3] = {Dn.j_b_x, Dn.j_b_y, Dn.j_b_z};
+    double t4 = p_reg(na) * cccoeff;
+    for (int d = 0; d < CODEDIM; d++) Aa[d][i] = (t4 == 0.0) ? 0.0 : t4 * (1. - af) * ja[d][i] / na;
+    t4 = p_reg(nb) * cccoeff;
+    for (int d = 0; d < CODEDIM; d++) Ab[d][i] = (t4 == 0.0) ? 0.0 : t4 * (1. - af) * jb[d][i] / nb;
+#endif
+    /* kinetic (Galilean) and mean-field contributions */
+    Va_const += af_p * (taua + taub) / 2.;
+    Vb_const += af_p * (taua + taub) / 2.;
+    Va_const += beta * eF;
+    Vb_const += beta * eF;
+#ifdef CURRENT_CORRECTIONS
+    {
+        double ja2 = 0.0, jb2 = 0.0;
+        for (int d = 0; d < CODEDIM; d++) { ja2 += ja[d][i] * ja[d][i]; jb2 += jb[d][i] * jb[d][i]; }
+        double t7 = p_reg(na) * cccoeff;
+        if (t7 != 0.0) {
+            t7 = t7 * ja2 / (2.0 * na);
+            Va_const += ((af - 1.0) / na - af_p) * t7;
+            Va_const -= cccoeff * dp_reg(na) * (af - 1.0) * ja2 / (2.0 * na);
+            Vb_const -= af_p * t7;
+        }
+        t7 = p_reg(nb) * cccoeff;
+        if (t7 != 0.0) {
+            t7 = t7 * jb2 / (2.0 * nb);
+            Va_const -= af_p * t7;
+            Vb_const += ((af - 1.0) / nb - af_p) * t7;
+            Vb_const -= cccoeff * dp_reg(nb) * (af - 1.0) * jb2 / (2.0 * nb);
+        }
+    }
+#endif
+#ifdef INCLUDE_MF_CORRECTION_FROM_REG_SCHEME
+    double lkF = std::pow(3.0 * M_PI * M_PI * (na + nb), 1.0 / 3.0);
+#endif
+    for (int k = 0; k < UD_SCITERS; k++) {
+        double lmu_sc = (dc_mu_a - Va + dc_mu_b - Vb) / 2.;
+        Complex p0 = std::sqrt(Complex(2.0 * lmu_sc / af, 0.0));
+        if (p0.imag() < 0.) p0 *= -1.;
+#ifdef USE_CUBIC_CUTOFF
+        Complex kc = Complex(M_PI / DX, 0.0);
+#else
+        Complex kc = std::sqrt(Complex(2.0 * (dc_ec + lmu_sc) / af, 0.0));
+        if (kc.imag() < 0.) kc *= -1.;
+#endif
+        Complex wz = std::log((kc + p0) / (kc - p0));
+        if (wz.imag() < 0.) wz += Complex(0.0, 2. * M_PI);
+        wz = kc * REG_COEFF_R0 * (1. - (p0 / kc) * REG_COEFF_R1 * wz);
+        double lambda = wz.real();
+        double g_eff = af / (ctilde - lambda);
+        ldelta = -lnu * g_eff;
+        double ddn = (std::conj(ldelta) * lnu).real();
+        double das = ldelta.real() * ldelta.real() + ldelta.imag() * ldelta.imag();
+        double Vanew = Va_const - (af_p / af) * ddn - ctilde_p / af * das;
+        double Vbnew = Vb_const - (af_p / af) * ddn - ctilde_p / af * das;
+#ifdef INCLUDE_MF_CORRECTION_FROM_REG_SCHEME
+        {
+            double bcoeff = (p0 / (lkF + 1.0e-12)).real();
+            double lx = bcoeff * lkF * DX / M_PI;
+            if (g_eff < -1.0e-10 && lx > 1.0e-10) {
+                double L0 = bcoeff * REG_COEFF_R0 / lx * (1.0 - REG_COEFF_R1 * lx * std::log((1.0 + lx) / (1.0 - lx)));
+                double dL0 = (-2. * bcoeff * REG_COEFF_R0 * REG_COEFF_R1) / (1. - lx * lx) - bcoeff * REG_COEFF_R0 / lx / lx;
+                double dLdn = (lkF / (3. * (na + nb) * af)) * (L0 + dL0 * bcoeff * DX * lkF / M_PI);
+                Vanew += dLdn * das;
+                Vbnew += dLdn * das;
+            }
+        }
+#endif
+        Va = UD_MIX_COEFF * Vanew + (1. - UD_MIX_COEFF) * Va;
+        Vb = UD_MIX_COEFF * Vbnew + (1. - UD_MIX_COEFF) * Vb;
+    }
     P.V_a[i] = Va; P.V_b[i] = Vb; P.delta[i] = ldelta;
 }
 #endif
@@ -1145,6 +1257,17 @@ int orc_energy(double *E)
 #if FUNCTIONAL == BDG
         e[EKIN * (size_t)N + i] = 0.5 * (P.alpha_a[i] * taua + P.alpha_b[i] * taub) * VOL;
         e[EPOT * (size_t)N + i] = 0.0;
+#elif FUNCTIONAL == SLDAE
+        /* tdwslda_functionals.h:815-884 */
+        {
+            double nt = na + nb;
+            double kF = std::pow(3. * std::pow(M_PI, 2) * nt, 1. / 3.);
+            double eF = std::pow(kF, 2) / 2.;
+            double x = std::fabs(scattering_length(ix, iy, iz, it, dc_params, dc_extra_data_size, dc_extra_data) * kF);
+            double af = osldae::a_functional_d0(x), bf = osldae::b_functional_d0(x);
+            e[EKIN * (size_t)N + i] = af * (taua + taub) / 2. * VOL;
+            e[EPOT * (size_t)N + i] = (3. / 5.) * bf * eF * nt * VOL;
+        }
 #else
         double p = pol(na, nb);
         e[EKIN * (size_t)N + i] = 0.5 * (alpha(p) * taua + alpha(-p) * taub) * VOL;
@@ -1209,6 +1332,18 @@ int orc_qf_densities(double *out)
     derivatives(y, 0);
     calculate_qf_densities(y);
     std::memcpy(out, dens.data() + 12 * (size_t)N, (size_t)4 * N * sizeof(double));
+    return 0;
+}
+/* densities of a weighted subset of the current states, with gradients and tau (pca.c:1056-1066,
+ * the subset tracking of md.subsetMinEn/subsetMaxEn) into out (12 N); summed over ranks */
+int orc_subset_densities(const double *weights, double *out)
+{
+    std::vector<double> d((size_t)16 * N, 0.0);
+    derivatives(y, 1);
+    calculate_densities(y, 1, weights, d.data());
+    if (xfn) xfn(xuser, d.data(), (size_t)12 * N);
+    density_tau(d.data());
+    std::memcpy(out, d.data(), (size_t)12 * N * sizeof(double));
     return 0;
 }
 int orc_set_quantum_friction(double alpha, double beta, double gamma, double nreq, double start, double stop, double ramp)

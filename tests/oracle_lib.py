@@ -61,6 +61,7 @@ class Oracle:
         L.orc_selfstart.restype = ctypes.c_int
         L.orc_set_quantum_friction.argtypes = [ctypes.c_double] * 7
         L.orc_qf_densities.argtypes = [_dp]
+        L.orc_subset_densities.argtypes = [_dp, _dp]
         L.orc_filter_field.argtypes = [_dp]
         self._xfn = None
         # the library is shared by every instance in the process: start from a plain run
@@ -92,6 +93,12 @@ class Oracle:
 
     def selfstart(self):
         return self.lib.orc_selfstart()
+
+    def subset_densities(self, weights):
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        a = np.zeros(12 * self.N)
+        self.lib.orc_subset_densities(_p(w), _p(a))
+        return a
 
     def qf_densities(self):
         a = np.zeros(4 * self.N)

@@ -123,3 +123,29 @@ def test_quantum_friction(has_gpu, name, nwf, nsteps, nmeas):
     assert rel(g["states"], o["states"]) < TOL
     assert rel(g["qpe"], o["qpe"]) < TOL
     assert rel(g["history0"], o["history"][0]) < TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,nwf", [("t2d_slda", 24), ("t3d_aslda", 24), ("c3_aslda3d", 8), ("t1d_custom", 24)])
+def test_subset_densities(has_gpu, name, nwf):
+    """densities of a weighted subset of the states after a few steps (subset tracking,
+    pca.c:1056-1066) against the oracle's calculate_densities with the same weights"""
+    from oracle_lib import Oracle
+    from wslda_b200 import TDRun
+    from parity_util import inputs
+    proj, d = inputs(name, nwf)
+    weights = (np.arange(nwf) % 3 == 0).astype(float)
+    weights[1] = 0.5
+    o = Oracle(name)
+    o.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+    o.initial_measurement()
+    o.steps(2)
+    want = o.subset_densities(weights)
+    r = TDRun(name, nwf)
+    r.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+    r.initial_measurement()
+    r.steps(2)
+    got = r.subset_densities(weights)
+    r.close()
+    for k, v in density_errors(got, want, proj.numel).items():
+        assert v < TOL, f"{name} subset density {k}: rel err {v:.3e}"

@@ -40,6 +40,7 @@ SIGNATURES = {
     "wtd_initial_measurement": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "wtd_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "wtd_selfstart": (ctypes.c_int, [ctypes.c_void_p]),
+    "wtd_subset_densities": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
     "wtd_energy": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "wtd_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "wtd_time_index": (ctypes.c_int, [ctypes.c_void_p]),
@@ -141,6 +142,13 @@ class TDRun:
 
     def initial_measurement(self, it0=None):
         self._check(self.lib.wtd_initial_measurement(self.h, int(self.it0 if it0 is None else it0)))
+
+    def subset_densities(self, weights):
+        """densities (12 N) of the states weighted by weights (subset tracking)"""
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        out = np.zeros(12 * self.N)
+        self._check(self.lib.wtd_subset_densities(self.h, _p(w), _p(out)))
+        return out
 
     def selfstart(self):
         """Taylor self-start of the ABM history (after initial_measurement)"""

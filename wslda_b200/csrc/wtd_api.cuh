@@ -1247,6 +1247,62 @@ extern "C" int wtd_selfstart(wtd_ctx *c)
     return r ? r : wtd_cuerr(cudaGetLastError());
 }
 
+/* densities of a weighted subset of the states (the reference's subset tracking, pca.c:842-870,
+ * 1056-1066: weight 1 for quasiparticle energies inside [subsetMinEn, subsetMaxEn] eF): the
+ * density sums of calculate_densities with each state's occupation factors multiplied by its
+ * weight (pca_dens.cu:46-47), gradients and tau included, summed over ranks */
+extern "C" int wtd_subset_densities(wtd_ctx *c, const double *weights, double *host12)
+{
+    if (!c || !weights || !host12) return WTD_ERR_ARG;
+    if (c->prec != WTD_FP64) return WTD_ERR_UNSUPPORTED;
+    WTD_CU(cudaSetDevice(c->dev));
+    constexpr size_t N = WTD_NUMEL;
+    const size_t NS = (size_t)2 * c->S * N;
+    SelfWork w{};
+    double *dw = NULL, *out = NULL;
+    auto get = [&](void **p, size_t bytes) -> int {
+        if (cudaMalloc(p, bytes) != cudaSuccess) { cudaGetLastError(); return WTD_ERR_NOMEM; }
+        w.own.push_back(*p);
+        return WTD_OK;
+    };
+    int r = WTD_OK;
+    if (c->staged) {
+        w.ddx = c->ddx; w.ddy = c->ddy; w.ddz = c->ddz; w.dlap = c->dlap;
+    } else {
+        r = get((void **)&w.ddx, NS * sizeof(double2));
+        if (!r && CODEDIM >= 2) r = get((void **)&w.ddy, NS * sizeof(double2));
+        if (!r && CODEDIM >= 3) r = get((void **)&w.ddz, NS * sizeof(double2));
+        if (!r) r = get((void **)&w.dlap, NS * sizeof(double2));
+    }
+    if (!r) r = get((void **)&dw, c->S * sizeof(double));
+    if (!r) r = get((void **)&out, 12 * N * sizeof(double));
+    if (!r) r = wtd_cuerr(cudaMemcpyAsync(dw, weights, c->S * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    if (!r) r = ss_derivs(c, w, (const double2 *)c->y, 1);
+    if (!r) {
+        k_dens_compat<<<c->grid, 256, 0, c->st>>>(c->S, (const double2 *)c->y, w.ddx, w.ddy, w.ddz, w.dlap, c->occ, dw,
+                                                  c->kp2, c->wcnt, c->dslot, 1);
+        wtd_dens_reduce<<<(12 * (int)N + 255) / 256, 256, 0, c->st>>>(c->dslot, c->grid, out, (int)N, 1, 1.0 / WTD_LPERP);
+        r = wtd_cuerr(cudaGetLastError());
+        c->launches += 2;
+    }
+    if (!r) r = exchange(c, out, 12 * N);
+    if (!r) {
+        if (WTD_BIG) {
+            r = big_tau(out, c->stage3d, c->tw, c->ktab, c->st);
+        } else {
+            constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
+            cudaFuncSetAttribute(wtd_tau_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            wtd_tau_kernel<WG><<<2, 512, sm, c->st>>>(out, c->tw, c->ktab);
+            r = wtd_cuerr(cudaGetLastError());
+            c->launches++;
+        }
+    }
+    if (!r) r = wtd_cuerr(cudaMemcpyAsync(host12, out, 12 * N * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    cudaStreamSynchronize(c->st);
+    for (void *q : w.own) cudaFree(q);
+    return r;
+}
+
 /* ---------------------------------------------------------------------------------------
  * adjoint (gradient of a loss of the final pairing field with respect to the parameters of
  * the external potential): forward with checkpoints, the last segment recorded as it runs;
