@@ -1,6 +1,6 @@
 /*
  * ORACLE (test infrastructure only).  SLDA/ASLDA energy density functional pieces, restated
- * from hpc-engine/pca_edf.h (line numbers cited per function).  A0..A2, G0, G1, GAMMA0,
+ * from hpc-engine/pca_edf.h (line numbers cited per function), and the SLDAE parameter fits.  A0..A2, G0, G1, GAMMA0,
  * P_NMIN/P_NMAX/P_ALPHA come from the project's settings (wtd_settings.h).
  */
 #ifndef ORACLE_EDF_H
@@ -107,4 +107,45 @@ static inline double dtC_db(double a, double b)
             (1.0 / 3.0) * alpha_plus(pol(a, b)) * std::pow(a + b + DENSEPSILON, -2.0 / 3.0)) / GAMMA0;
 }
 } // namespace oedf
+
+#if FUNCTIONAL == SLDAE
+/* SLDAE parameter fits (hpc-engine/sldae_functional.c:68-330): Pade[4/4] forms in x = |a kF|,
+ * written term by term as the reference does; the coefficient tables come from wtd_settings.h */
+namespace osldae {
+static inline double pade_num(double x, const double *a) { return a[0] * x + a[1] * x * x + a[2] * std::pow(x, 3) + a[3] * std::pow(x, 4); }
+static inline double pade_den(double x, const double *b) { return 1. + b[0] * x + b[1] * x * x + b[2] * std::pow(x, 3) + b[3] * std::pow(x, 4); }
+/* sldae_functional.c:68-72 */
+static inline double pade_d0(double x, const double *a, const double *b) { return pade_num(x, a) / pade_den(x, b); }
+/* sldae_functional.c:74-80 */
+static inline double pade_d1(double x, const double *a, const double *b)
+{
+    double dn = a[0] + 2. * a[1] * x + 3. * a[2] * x * x + 4. * a[3] * std::pow(x, 3);
+    double dd = b[0] + 2. * b[1] * x + 3. * b[2] * x * x + 4. * b[3] * std::pow(x, 3);
+    double d = pade_den(x, b);
+    return -(dd * pade_num(x, a)) / (d * d) + dn / d;
+}
+static const double AL_A[4] = {0.0, WTD_SLDAE_ALPHA_A2, WTD_SLDAE_ALPHA_A3, WTD_SLDAE_ALPHA_A4};
+static const double AL_B[4] = {WTD_SLDAE_ALPHA_B1, WTD_SLDAE_ALPHA_B2, WTD_SLDAE_ALPHA_B3, WTD_SLDAE_ALPHA_B4};
+static const double BE_A[4] = {SLDAE_beta_a1, SLDAE_beta_a2, SLDAE_beta_a3, SLDAE_beta_c};
+static const double BE_B[4] = {SLDAE_beta_b1, SLDAE_beta_b2, SLDAE_beta_b3, SLDAE_beta_c};
+static const double IG_A[4] = {SLDAE_inverse_gamma_a1, SLDAE_inverse_gamma_a2, SLDAE_inverse_gamma_a3, SLDAE_inverse_gamma_c};
+static const double IG_B[4] = {SLDAE_inverse_gamma_b1, SLDAE_inverse_gamma_b2, SLDAE_inverse_gamma_b3, SLDAE_inverse_gamma_c};
+static const double BF_A[4] = {SLDAE_b_functional_a1, SLDAE_b_functional_a2, SLDAE_b_functional_a3, SLDAE_b_functional_c};
+static const double BF_B[4] = {SLDAE_b_functional_b1, SLDAE_b_functional_b2, SLDAE_b_functional_b3, SLDAE_b_functional_c};
+static const double CF_A[4] = {SLDAE_c_functional_a1, SLDAE_c_functional_a2, SLDAE_c_functional_a3, SLDAE_c_functional_c};
+static const double CF_B[4] = {SLDAE_c_functional_b1, SLDAE_c_functional_b2, SLDAE_c_functional_b3, SLDAE_c_functional_c};
+#ifdef SLDA_FORCE_A1
+static inline double alpha_d0(double) { return 1.; }
+static inline double alpha_d1(double) { return 0.; }
+#else
+static inline double alpha_d0(double x) { return 1. + pade_d0(x, AL_A, AL_B); }
+static inline double alpha_d1(double x) { return pade_d1(x, AL_A, AL_B); }
+#endif
+static inline double beta_d0(double x) { return BF_APS_UFG * pade_d0(x, BE_A, BE_B); }
+static inline double inverse_gamma_d0(double x) { return (1. / CF_APS_UFG) * pade_d0(x, IG_A, IG_B); }
+static inline double a_functional_d0(double x) { return alpha_d0(x); }
+static inline double b_functional_d0(double x) { return BF_APS_UFG * pade_d0(x, BF_A, BF_B); }
+static inline double c_functional_d0(double x) { return CF_APS_UFG * pade_d0(x, CF_A, CF_B); }
+} // namespace osldae
+#endif
 #endif

@@ -36,6 +36,9 @@ CASES = {
     "t2d_vext": (24, 3, 2, True),
     "t1d_bdg_vext": (24, 3, 2, True),
     "t2d_big": (8, 3, 1, False),
+    "t2d_sldae": (24, 3, 2, True),
+    "t3d_sldae": (24, 3, 2, True),
+    "t1d_sldae_a1": (24, 3, 2, True),
 }
 
 # effective-mass filter cases (pca.c:1448-1453, hkf_mode 1): the same runs with alpha_a,

@@ -156,7 +156,8 @@ def run_compat(name, nwf, nsteps, nmeas):
 
 
 SMALL = ["t1d_custom", "t1d_aslda", "t2d_slda", "t2d_bdg", "t3d_slda", "t3d_aslda", "c1_bdg1d", "c4_bdg2d",
-         "c2_slda2d", "c3_aslda3d", "c5_slda3d", "t2d_vext", "t1d_bdg_vext", "t2d_big"]
+         "c2_slda2d", "c3_aslda3d", "c5_slda3d", "t2d_vext", "t1d_bdg_vext", "t2d_big", "t2d_sldae", "t3d_sldae",
+         "t1d_sldae_a1"]
 
 
 @pytest.mark.gpu

@@ -1,6 +1,6 @@
 """CUDA library vs the CPU oracle on the same seeded inputs (FP64 form: 1e-10 relative).
 
-Every small project (1D/2D/3D, CUSTOMEDF / SLDA / ASLDA / BDG, AB3AM4 / AB4AM5 / AB5AM5, radix
+Every small project (1D/2D/3D, CUSTOMEDF / SLDA / ASLDA / BDG / SLDAE, AB3AM4 / AB4AM5 / AB5AM5, radix
 2/3/4/8 lattices) is advanced through two measurement blocks, so both the plain steps and the
 gradient (tau, j) steps are covered; then densities, potentials, energy terms, particle
 numbers, quasiparticle energies and the states themselves are compared.
@@ -11,7 +11,8 @@ import pytest
 from parity_util import density_errors, rel, run_gpu, run_oracle
 
 TOL = 1e-10
-SMALL = ["t1d_custom", "t1d_aslda", "t2d_slda", "t2d_bdg", "t3d_slda", "t3d_aslda", "t2d_vext", "t1d_bdg_vext"]
+SMALL = ["t1d_custom", "t1d_aslda", "t2d_slda", "t2d_bdg", "t3d_slda", "t3d_aslda", "t2d_vext", "t1d_bdg_vext",
+         "t2d_sldae", "t3d_sldae", "t1d_sldae_a1"]
 
 
 def _compare(name, nwf, nsteps, nmeas, tol=TOL, hkf=None):

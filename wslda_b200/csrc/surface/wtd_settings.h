@@ -52,7 +52,83 @@
 #endif
 
 #if FUNCTIONAL==SLDAE
-#error "FUNCTIONAL SLDAE is not provided by this library"
+/* SLDAE: the published Pade[4/4] fits of the extended SLDA functional of Boulet et al.
+ * (hpc-engine/sldae_parameters.h, sldae_parameters_A1.h, sldae_functional.c:93-330).  Each
+ * parameter is P(x) = s * (a1 x + a2 x^2 + a3 x^3 + a4 x^4) / (1 + b1 x + b2 x^2 + b3 x^3 + b4 x^4)
+ * of x = |a kF|, with a4 = b4 = c for the fitted sets.  The effective-mass fit alpha(x) =
+ * 1 + P(x) is the same for both sets and becomes alpha = 1 under SLDA_FORCE_A1. */
+#define WTD_SLDAE_ALPHA_A2 (-0.2081560)
+#define WTD_SLDAE_ALPHA_A3 (-0.1358830)
+#define WTD_SLDAE_ALPHA_A4 (-0.0162071)
+#define WTD_SLDAE_ALPHA_B1 (2.09838000)
+#define WTD_SLDAE_ALPHA_B2 (1.73800000)
+#define WTD_SLDAE_ALPHA_B3 (0.66854900)
+#define WTD_SLDAE_ALPHA_B4 (0.10150800)
+#ifdef SLDA_FORCE_A1
+#define SLDAE_beta_a1 +0.797400
+#define SLDAE_beta_a2 +0.943961
+#define SLDAE_beta_a3 +1.037043
+#define SLDAE_beta_b1 +1.227062
+#define SLDAE_beta_b2 +2.126210
+#define SLDAE_beta_b3 +1.734795
+#define SLDAE_beta_c  +0.523445
+#define SLDAE_b_functional_a1 +0.698112
+#define SLDAE_b_functional_a2 +0.034678
+#define SLDAE_b_functional_a3 +0.455138
+#define SLDAE_b_functional_b1 +0.353905
+#define SLDAE_b_functional_b2 +0.806444
+#define SLDAE_b_functional_b3 +0.403679
+#define SLDAE_b_functional_c  -0.031327
+#define SLDAE_inverse_gamma_a1 +2.713374
+#define SLDAE_inverse_gamma_a2 +1.441196
+#define SLDAE_inverse_gamma_a3 +3.700251
+#define SLDAE_inverse_gamma_b1 +0.634303
+#define SLDAE_inverse_gamma_b2 +3.522427
+#define SLDAE_inverse_gamma_b3 +3.701347
+#define SLDAE_inverse_gamma_c  +1.877961
+#define SLDAE_c_functional_a1 +0.370145
+#define SLDAE_c_functional_a2 +1.041299
+#define SLDAE_c_functional_a3 +1.737347
+#define SLDAE_c_functional_b1 +2.458364
+#define SLDAE_c_functional_b2 +5.604947
+#define SLDAE_c_functional_b3 +3.828124
+#define SLDAE_c_functional_c  +1.085400
+#define AF_APS_UFG +1.000000
+#define BF_APS_UFG -0.481506
+#define CF_APS_UFG -10.532397
+#else
+#define SLDAE_beta_a1 +1.58442
+#define SLDAE_beta_a2 +17.2973
+#define SLDAE_beta_a3 +0.820671
+#define SLDAE_beta_b1 +13.9448
+#define SLDAE_beta_b2 +10.1914
+#define SLDAE_beta_b3 +11.9429
+#define SLDAE_beta_c  +3.48966
+#define SLDAE_b_functional_a1 +1.29871
+#define SLDAE_b_functional_a2 +6.02212
+#define SLDAE_b_functional_a3 +0.376541
+#define SLDAE_b_functional_b1 +6.47079
+#define SLDAE_b_functional_b2 +3.73389
+#define SLDAE_b_functional_b3 +3.47301
+#define SLDAE_b_functional_c  +0.810972
+#define SLDAE_inverse_gamma_a1 +6.15853
+#define SLDAE_inverse_gamma_a2 +0.156722
+#define SLDAE_inverse_gamma_a3 +0.76668
+#define SLDAE_inverse_gamma_b1 +1.48431
+#define SLDAE_inverse_gamma_b2 +2.07468
+#define SLDAE_inverse_gamma_b3 +0.737836
+#define SLDAE_inverse_gamma_c  +0.0823379
+#define SLDAE_c_functional_a1 +0.267952
+#define SLDAE_c_functional_a2 +0.754923
+#define SLDAE_c_functional_a3 +0.330699
+#define SLDAE_c_functional_b1 +2.61695
+#define SLDAE_c_functional_b2 +2.71855
+#define SLDAE_c_functional_b3 +0.550587
+#define SLDAE_c_functional_c  +0.0900897
+#define AF_APS_UFG (0.8403360)
+#define BF_APS_UFG (-0.281863)
+#define CF_APS_UFG (-14.95950)
+#endif
 #endif
 
 /* mode derivation (pca_settings.h:75-95, 186-222) */

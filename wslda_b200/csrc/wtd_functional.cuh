@@ -5,6 +5,8 @@
  *   SLDA / ASLDA  hpc-engine/tdwslda_functionals.h:47-306 (potentials), :308-366 (energy),
  *                 EDF pieces hpc-engine/pca_edf.h:17-350
  *   BDG           hpc-engine/tdwslda_functionals.h:373-452 (potentials), :455-503 (energy)
+ *   SLDAE         hpc-engine/tdwslda_functionals.h:530-812 (potentials), :815-884 (energy),
+ *                 parameter fits hpc-engine/sldae_functional.c:68-330
  *   CUSTOMEDF     the user's tdwslda_compute_potentials / tdwslda_compute_energy kernels from
  *                 problem-definition.h, launched unchanged
  *
@@ -120,6 +122,59 @@ __device__ __forceinline__ double dtildeC(double a, double b, bool wrt_a)
             (1.0 / 3.0) * alpha_plus(pol(a, b)) * pow(a + b + DENSEPSILON, -2.0 / 3.0)) / GAMMA0;
 }
 } // namespace edf
+
+#if FUNCTIONAL == SLDAE
+namespace sldae {
+/* Pade[4/4] form P(x) = N(x)/D(x) of the SLDAE parameter fits and its first derivative
+ * (sldae_functional.c:68-80), evaluated in Horner form */
+__device__ __forceinline__ double pade0(double x, double a1, double a2, double a3, double a4,
+                                        double b1, double b2, double b3, double b4)
+{
+    double num = x * (a1 + x * (a2 + x * (a3 + x * a4)));
+    double den = 1.0 + x * (b1 + x * (b2 + x * (b3 + x * b4)));
+    return num / den;
+}
+__device__ __forceinline__ double pade1(double x, double a1, double a2, double a3, double a4,
+                                        double b1, double b2, double b3, double b4)
+{
+    double num = x * (a1 + x * (a2 + x * (a3 + x * a4)));
+    double dnum = a1 + x * (2.0 * a2 + x * (3.0 * a3 + x * (4.0 * a4)));
+    double den = 1.0 + x * (b1 + x * (b2 + x * (b3 + x * b4)));
+    double dden = b1 + x * (2.0 * b2 + x * (3.0 * b3 + x * (4.0 * b4)));
+    return (dnum * den - num * dden) / (den * den);
+}
+#define WTD_SLDAE_ALPHA_SET 0.0, WTD_SLDAE_ALPHA_A2, WTD_SLDAE_ALPHA_A3, WTD_SLDAE_ALPHA_A4, \
+    WTD_SLDAE_ALPHA_B1, WTD_SLDAE_ALPHA_B2, WTD_SLDAE_ALPHA_B3, WTD_SLDAE_ALPHA_B4
+#define WTD_SLDAE_SET(p) p##_a1, p##_a2, p##_a3, p##_c, p##_b1, p##_b2, p##_b3, p##_c
+/* effective mass alpha(x) = a(x) (sldae_functional.c:93-166, 264-284) */
+__device__ __forceinline__ double a_functional(double x)
+{
+#ifdef SLDA_FORCE_A1
+    return 1.0;
+#else
+    return 1.0 + pade0(x, WTD_SLDAE_ALPHA_SET);
+#endif
+}
+__device__ __forceinline__ double a_functional_d1(double x)
+{
+#ifdef SLDA_FORCE_A1
+    return 0.0;
+#else
+    return pade1(x, WTD_SLDAE_ALPHA_SET);
+#endif
+}
+/* beta, 1/gamma, b and c (sldae_functional.c:168-262, 286-330) */
+__device__ __forceinline__ double beta(double x) { return BF_APS_UFG * pade0(x, WTD_SLDAE_SET(SLDAE_beta)); }
+__device__ __forceinline__ double inverse_gamma(double x)
+{
+    return (1. / CF_APS_UFG) * pade0(x, WTD_SLDAE_SET(SLDAE_inverse_gamma));
+}
+__device__ __forceinline__ double b_functional(double x) { return BF_APS_UFG * pade0(x, WTD_SLDAE_SET(SLDAE_b_functional)); }
+__device__ __forceinline__ double c_functional(double x) { return CF_APS_UFG * pade0(x, WTD_SLDAE_SET(SLDAE_c_functional)); }
+/* x = |a kF| at one point, kF = (3 pi^2 n)^(1/3) */
+__device__ __forceinline__ double kfermi(double nt) { return pow(3. * (M_PI * M_PI) * nt, 1. / 3.); }
+} // namespace sldae
+#endif
 
 #if FUNCTIONAL == SLDA || FUNCTIONAL == ASLDA
 /* tdwslda_functionals.h:47-306 */
@@ -313,6 +368,145 @@ __global__ void wtd_energy_kernel(int it, wslda_density Dn, wslda_potential P, d
     tb -= p_reg(nb) * (x2 * x2 + y2 * y2 + z2 * z2) / nb;
     Ek[i] = 0.5 * (P.alpha_a[i] * ta + P.alpha_b[i] * tb) * WTD_VOLEL;
     Ep[i] = 0.0;
+    Epair[i] = (P.delta[i] * thrust::conj(Dn.nu[i])).real() * (-1.0) * WTD_VOLEL;
+    Ec[i] = p_reg(na) * (x1 * x1 + y1 * y1 + z1 * z1) / (2. * na) * WTD_VOLEL +
+            p_reg(nb) * (x2 * x2 + y2 * y2 + z2 * z2) / (2. * nb) * WTD_VOLEL;
+}
+#elif FUNCTIONAL == SLDAE
+/* tdwslda_functionals.h:530-812: spin-symmetric parameters a, b, c of x = |a kF|, the
+ * current-correction terms with alpha_a = alpha_b = a(x), and the local self-consistent
+ * solution for U and Delta with g_eff = a / (c~ - Lambda) */
+__global__ void wtd_potentials_kernel(int it, wslda_density Dn, wslda_potential P, double cccoeff)
+{
+    using namespace edf;
+    using namespace sldae;
+    int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i >= WTD_NUMEL) return;
+    int ix, iy, iz; wtd_decode(i, ix, iy, iz);
+    double Va_c = WTD_U_EXT(ix, iy, iz, it, SPINA);
+    double Vb_c = WTD_U_EXT(ix, iy, iz, it, SPINB);
+    double na = Dn.rho_a[i], nb = Dn.rho_b[i];
+    double ta = Dn.tau_a[i], tb = Dn.tau_b[i];
+    double nt = na + nb;
+    double n13 = pow(nt, 1. / 3.), n23 = pow(nt, 2. / 3.);
+    double kF = kfermi(nt), eF = kF * kF / 2.;
+    double x = fabs(scattering_length(ix, iy, iz, it, dc_params, dc_extra_data_size, dc_extra_data) * kF);
+    double nreg = p_reg(nt);
+    double bet = beta(x), ig = inverse_gamma(x);
+    double af = a_functional(x), cf = c_functional(x);
+    double af_p = 0.0, cf_p = 0.0;
+    if (nreg > 0.0) {
+        af_p = nreg * x / (3. * nt) * a_functional_d1(x);
+        cf_p = nreg * cf / (3. * nt) * (1. - cf * ig);
+    }
+    double ct = af * n13 / cf;
+    double igeff = (1 / cf) * (1. - 3. * nt / cf * cf_p);
+    double ct_p = (nreg > 0.) ? pow(nreg, 2. / 3.) * igeff * af / (3. * n23) : 0.;
+    ct_p += af_p * n13 / cf;
+#ifdef CURRENT_CORRECTIONS
+    P.alpha_a[i] = af; P.alpha_b[i] = af;
+    double jx = Dn.j_a_x[i], kx = Dn.j_b_x[i];
+    double jy = (CODEDIM >= 2) ? Dn.j_a_y[i] : 0.0, ky = (CODEDIM >= 2) ? Dn.j_b_y[i] : 0.0;
+    double jz = (CODEDIM >= 3) ? Dn.j_a_z[i] : 0.0, kz = (CODEDIM >= 3) ? Dn.j_b_z[i] : 0.0;
+    {
+        double t4 = p_reg(na) * cccoeff;
+        P.A_a_x[i] = (t4 == 0.0) ? 0.0 : t4 * (1. - af) * jx / na;
+        if (CODEDIM >= 2) P.A_a_y[i] = (t4 == 0.0) ? 0.0 : t4 * (1. - af) * jy / na;
+        if (CODEDIM >= 3) P.A_a_z[i] = (t4 == 0.0) ? 0.0 : t4 * (1. - af) * jz / na;
+        t4 = p_reg(nb) * cccoeff;
+        P.A_b_x[i] = (t4 == 0.0) ? 0.0 : t4 * (1. - af) * kx / nb;
+        if (CODEDIM >= 2) P.A_b_y[i] = (t4 == 0.0) ? 0.0 : t4 * (1. - af) * ky / nb;
+        if (CODEDIM >= 3) P.A_b_z[i] = (t4 == 0.0) ? 0.0 : t4 * (1. - af) * kz / nb;
+    }
+#endif
+    Va_c += af_p * (ta + tb) / 2.;
+    Vb_c += af_p * (ta + tb) / 2.;
+    Va_c += bet * eF;
+    Vb_c += bet * eF;
+#ifdef CURRENT_CORRECTIONS
+    {
+        double t7 = p_reg(na) * cccoeff;
+        if (t7 != 0.0) {
+            double j2 = jx * jx + jy * jy + jz * jz;
+            t7 = t7 * j2 / (2.0 * na);
+            Va_c += ((af - 1.0) / na - af_p) * t7;
+            Va_c -= cccoeff * dp_reg(na) * (af - 1.0) * j2 / (2.0 * na);
+            Vb_c -= af_p * t7;
+        }
+        t7 = p_reg(nb) * cccoeff;
+        if (t7 != 0.0) {
+            double k2 = kx * kx + ky * ky + kz * kz;
+            t7 = t7 * k2 / (2.0 * nb);
+            Va_c -= af_p * t7;
+            Vb_c += ((af - 1.0) / nb - af_p) * t7;
+            Vb_c -= cccoeff * dp_reg(nb) * (af - 1.0) * k2 / (2.0 * nb);
+        }
+    }
+#endif
+    double Va = P.V_a[i], Vb = P.V_b[i];
+    Complex lnu = Dn.nu[i], ld = P.delta[i], p0, kc, wz;
+#ifdef INCLUDE_MF_CORRECTION_FROM_REG_SCHEME
+    double lkF = pow(3.0 * M_PI * M_PI * (na + nb), 1.0 / 3.0);
+#endif
+    for (int k = 0; k < UD_SCITERS; k++) {
+        double lmu = (dc_mu_a - Va + dc_mu_b - Vb) / 2.;
+        p0 = thrust::sqrt(Complex(2.0 * lmu / af, 0.0));
+        if (p0.imag() < 0.) p0 *= -1.;
+#ifdef USE_CUBIC_CUTOFF
+        kc = Complex(M_PI / DX, 0.0);
+#else
+        kc = thrust::sqrt(Complex(2.0 * (dc_ec + lmu) / af, 0.0));
+        if (kc.imag() < 0.) kc *= -1.;
+#endif
+        wz = thrust::log((kc + p0) / (kc - p0));
+        if (wz.imag() < 0.) wz += Complex(0.0, 2. * M_PI);
+        wz = kc * REG_COEFF_R0 * (1. - (p0 / kc) * REG_COEFF_R1 * wz);
+        double geff = af / (ct - wz.real());
+        ld = lnu * (-geff);
+        double dn = (thrust::conj(ld) * lnu).real();
+        double d2 = ld.real() * ld.real() + ld.imag() * ld.imag();
+        double Van = Va_c - (af_p / af) * dn - ct_p / af * d2;
+        double Vbn = Vb_c - (af_p / af) * dn - ct_p / af * d2;
+#ifdef INCLUDE_MF_CORRECTION_FROM_REG_SCHEME
+        {
+            double bc = (p0 / (lkF + 1.0e-12)).real();
+            double lx = bc * lkF * DX / M_PI;
+            if (geff < -1.0e-10 && lx > 1.0e-10) {
+                double L0 = bc * REG_COEFF_R0 / lx * (1.0 - REG_COEFF_R1 * lx * log((1.0 + lx) / (1.0 - lx)));
+                double dL0 = (-2. * bc * REG_COEFF_R0 * REG_COEFF_R1) / (1. - lx * lx) - bc * REG_COEFF_R0 / lx / lx;
+                double dLdn = (lkF / (3. * (na + nb) * af)) * (L0 + dL0 * bc * DX * lkF / M_PI);
+                Van += dLdn * d2;
+                Vbn += dLdn * d2;
+            }
+        }
+#endif
+        Va = UD_MIX_COEFF * Van + (1. - UD_MIX_COEFF) * Va;
+        Vb = UD_MIX_COEFF * Vbn + (1. - UD_MIX_COEFF) * Vb;
+    }
+    P.V_a[i] = Va; P.V_b[i] = Vb; P.delta[i] = ld;
+}
+
+/* tdwslda_functionals.h:815-884 */
+__global__ void wtd_energy_kernel(int it, wslda_density Dn, wslda_potential P, double *Ek, double *Ep, double *Epair, double *Ec)
+{
+    using namespace edf;
+    using namespace sldae;
+    int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i >= WTD_NUMEL) return;
+    int ix, iy, iz; wtd_decode(i, ix, iy, iz);
+    double na = Dn.rho_a[i], nb = Dn.rho_b[i];
+    double ta = Dn.tau_a[i], tb = Dn.tau_b[i];
+    double x1 = Dn.j_a_x[i], x2 = Dn.j_b_x[i];
+    double y1 = (CODEDIM >= 2) ? Dn.j_a_y[i] : 0.0, y2 = (CODEDIM >= 2) ? Dn.j_b_y[i] : 0.0;
+    double z1 = (CODEDIM >= 3) ? Dn.j_a_z[i] : 0.0, z2 = (CODEDIM >= 3) ? Dn.j_b_z[i] : 0.0;
+    ta -= p_reg(na) * (x1 * x1 + y1 * y1 + z1 * z1) / na;
+    tb -= p_reg(nb) * (x2 * x2 + y2 * y2 + z2 * z2) / nb;
+    double nt = na + nb;
+    double kF = kfermi(nt), eF = kF * kF / 2.;
+    double x = fabs(scattering_length(ix, iy, iz, it, dc_params, dc_extra_data_size, dc_extra_data) * kF);
+    double af = a_functional(x), bf = b_functional(x);
+    Ek[i] = af * (ta + tb) / 2. * WTD_VOLEL;
+    Ep[i] = (3. / 5.) * bf * eF * nt * WTD_VOLEL;
     Epair[i] = (P.delta[i] * thrust::conj(Dn.nu[i])).real() * (-1.0) * WTD_VOLEL;
     Ec[i] = p_reg(na) * (x1 * x1 + y1 * y1 + z1 * z1) / (2. * na) * WTD_VOLEL +
             p_reg(nb) * (x2 * x2 + y2 * y2 + z2 * z2) / (2. * nb) * WTD_VOLEL;

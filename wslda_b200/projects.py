@@ -54,7 +54,8 @@ class Project:
         self.scheme = pre.get("INTEGRATION_SCHEME", "AB4AM5")
         self.nhist = {"AB3AM4": 3, "AB4AM5": 4, "AB5AM5": 5}[self.scheme]
         # an external velocity field forces the variable-mass (current-correction) path
-        self.const_mass = bool((self.functional in ("SLDA", "BDG") or "SLDA_FORCE_A1" in pre)
+        self.const_mass = bool((self.functional in ("SLDA", "BDG") or "SLDA_FORCE_A1" in pre
+                                or "SLDAE_FORCE_A1" in pre)
                                and "ENABLE_VELOCITY_EXT" not in pre)
         self.dims = [self.nx, self.ny if self.codedim >= 2 else 1, self.nz if self.codedim >= 3 else 1]
         self.numel = int(np.prod(self.dims))
