@@ -36,6 +36,10 @@ int normalize_wf(int n, Z *wf, int nthreads);
 int compute_derivatives(int n, Z *wf, Z *dx, Z *dy, Z *dz, Z *lap, int nthreads);
 int compute_laplace(int n, Z *wf, Z *lap, int nthreads);
 int density_caculate_tau(double *dens, int nthreads);
+#ifdef SPINSYMMETRY_MODE
+int symmetrize_densities_device(double *d_densities);
+static int ref_symm(int rc, double *d) { return rc ? rc : symmetrize_densities_device(d); }
+#endif
 int compute_potentials(int it, double *dens, double *pots, double cccoeff, int nthreads);
 int multiply_wf_by_alpha(int n, Z *in, Z *out, double *pots, int nthreads);
 int compute_energy(int it, double *dens, double *pots, double *work, int nthreads);
@@ -233,7 +237,12 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
 #define HAPPLYW(it, in, out, uq) apply_hamiltonian(it, nwf, in, out, d_dx, d_kk, d_lap, d_alap, d_dens, d_pots, qfsw, uq, pcc, nthreads)
 #define QFDENS() calculate_quantum_friction_densities(nwf, d_wf, d_lap, d_kk, d_fb, NULL, d_cnt, d_dens + 12 * (size_t)RN, nthreads)
 #endif
+#ifdef SPINSYMMETRY_MODE
+    /* pca.c:954, 1137, 1439: the spin-symmetric densities are copied a -> b after the exchange */
+#define DENS(g) ref_symm(DENSW(d_wf, g), d_dens)
+#else
 #define DENS(g) DENSW(d_wf, g)
+#endif
 #define HAPPLY(it, out) HAPPLYW(it, d_wf, out, NULL)
 #define DERIVS(w, g) ((g) ? compute_derivatives(2 * nwf, w, d_dx, d_dy, d_dz, d_lap, nthreads) : compute_laplace(2 * nwf, w, d_lap, nthreads))
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE

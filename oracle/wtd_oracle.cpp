@@ -368,25 +368,38 @@ static void calculate_densities(std::vector<Complex> &w, int grads, const double
             wcnt = (double)cnt[n];
 #endif
             Complex u = U(w, n)[i], v = V(w, n)[i];
+#ifdef SPINSYMMETRY_MODE
+            /* spin-symmetric system (pca_dens.cu:55-62): the u and v contributions go to one
+             * channel, taken for both spins below; nu without the factor 1/2 */
+            nb += (std::norm(v) * fbmEn + std::norm(u) * fbEn) * wcnt;
+            nu += u * std::conj(v) * (fbmEn - fbEn) * wcnt;
+            double &tu = taub, &jux = jbx, &juy = jby, &juz = jbz;
+#else
             na += std::norm(u) * fbEn * wcnt;
             nb += std::norm(v) * fbmEn * wcnt;
             nu += u * std::conj(v) * (fbmEn - fbEn) / 2.0 * wcnt;
+            double &tu = taua, &jux = jax, &juy = jay, &juz = jaz;
+#endif
+            (void)juy; (void)juz;
             if (grads) {
                 Complex lu = U(dlap, n)[i], lv = V(dlap, n)[i];
-                taua += (std::conj(u) * (lu - u * kp2)).real() * fbEn * wcnt;
+                tu += (std::conj(u) * (lu - u * kp2)).real() * fbEn * wcnt;
                 taub += (std::conj(v) * (lv - v * kp2)).real() * fbmEn * wcnt;
-                jax += (std::conj(u) * U(ddx, n)[i]).imag() * fbEn * wcnt;
+                jux += (std::conj(u) * U(ddx, n)[i]).imag() * fbEn * wcnt;
                 jbx -= (std::conj(v) * V(ddx, n)[i]).imag() * fbmEn * wcnt;
 #if CODEDIM >= 2
-                jay += (std::conj(u) * U(ddy, n)[i]).imag() * fbEn * wcnt;
+                juy += (std::conj(u) * U(ddy, n)[i]).imag() * fbEn * wcnt;
                 jby -= (std::conj(v) * V(ddy, n)[i]).imag() * fbmEn * wcnt;
 #endif
 #if CODEDIM >= 3
-                jaz += (std::conj(u) * U(ddz, n)[i]).imag() * fbEn * wcnt;
+                juz += (std::conj(u) * U(ddz, n)[i]).imag() * fbEn * wcnt;
                 jbz -= (std::conj(v) * V(ddz, n)[i]).imag() * fbmEn * wcnt;
 #endif
             }
         }
+#ifdef SPINSYMMETRY_MODE
+        na = nb; taua = taub; jax = jbx; jay = jby; jaz = jbz;
+#endif
         const double L = WTD_LPERP;
         D.rho_a[i] = na / DF / L; D.rho_b[i] = nb / DF / L;
         D.tau_a[i] = taua / DF / L; D.tau_b[i] = taub / DF / L;
@@ -419,10 +432,19 @@ static void calculate_qf_densities(std::vector<Complex> &w)
 #endif
             Complex u = U(w, n)[i], v = V(w, n)[i];
             Complex lu = U(dlap, n)[i] - u * kp2, lv = V(dlap, n)[i] - v * kp2;
+#ifdef SPINSYMMETRY_MODE
+            /* pca_dens.cu:411-414 */
+            ub += ((std::conj(u) * lu).imag() * f - (std::conj(v) * lv).imag() * fm) * wcnt;
+            d += (std::conj(v) * lu + std::conj(lv) * u) * (fm - f) * wcnt * 2.0;
+#else
             ua += (std::conj(u) * lu).imag() * f * wcnt;
             ub -= (std::conj(v) * lv).imag() * fm * wcnt;
             d += (std::conj(v) * lu + std::conj(lv) * u) * (fm - f) * wcnt;
+#endif
         }
+#ifdef SPINSYMMETRY_MODE
+        ua = ub;
+#endif
         const double L = WTD_LPERP;
         Ua[i] = ua / L;
         Ub[i] = ub / L;

@@ -39,6 +39,9 @@ CASES = {
     "t2d_sldae": (24, 3, 2, True),
     "t3d_sldae": (24, 3, 2, True),
     "t1d_sldae_a1": (24, 3, 2, True),
+    "t2d_aslda_sym": (24, 3, 2, True),
+    "t3d_sldae_a1_sym": (24, 3, 2, True),
+    "t1d_bdg_sym": (24, 3, 2, True),
 }
 
 # effective-mass filter cases (pca.c:1448-1453, hkf_mode 1): the same runs with alpha_a,
@@ -73,6 +76,8 @@ QF_CASES = {
     "t1d_aslda": (24, 3, 2, True),
     "c4_bdg2d": (16, 4, 1, False),
     "t3d_aslda": (24, 3, 2, True),
+    "t2d_aslda_sym": (24, 3, 2, True),
+    "t1d_bdg_sym": (24, 3, 2, True),
 }
 QF_PARAMS = (0.5, 0.3, 0.2, 10.0, 0.0, 100.0, 0.02)
 

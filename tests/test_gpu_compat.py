@@ -157,7 +157,7 @@ def run_compat(name, nwf, nsteps, nmeas):
 
 SMALL = ["t1d_custom", "t1d_aslda", "t2d_slda", "t2d_bdg", "t3d_slda", "t3d_aslda", "c1_bdg1d", "c4_bdg2d",
          "c2_slda2d", "c3_aslda3d", "c5_slda3d", "t2d_vext", "t1d_bdg_vext", "t2d_big", "t2d_sldae", "t3d_sldae",
-         "t1d_sldae_a1"]
+         "t1d_sldae_a1", "t2d_aslda_sym", "t3d_sldae_a1_sym", "t1d_bdg_sym"]
 
 
 @pytest.mark.gpu
@@ -226,7 +226,7 @@ def test_compat_high_k_filters(has_gpu, name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["t1d_aslda", "t2d_slda", "t3d_aslda", "c4_bdg2d"])
+@pytest.mark.parametrize("name", ["t1d_aslda", "t2d_slda", "t3d_aslda", "c4_bdg2d", "t2d_aslda_sym", "t1d_bdg_sym"])
 def test_compat_quantum_friction_densities(has_gpu, name):
     """calculate_quantum_friction_densities (pca_dens.cu:431 and the 2D/1D forms) against the
     oracle on the normalised initial states"""

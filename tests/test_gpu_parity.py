@@ -12,7 +12,7 @@ from parity_util import density_errors, rel, run_gpu, run_oracle
 
 TOL = 1e-10
 SMALL = ["t1d_custom", "t1d_aslda", "t2d_slda", "t2d_bdg", "t3d_slda", "t3d_aslda", "t2d_vext", "t1d_bdg_vext",
-         "t2d_sldae", "t3d_sldae", "t1d_sldae_a1"]
+         "t2d_sldae", "t3d_sldae", "t1d_sldae_a1", "t2d_aslda_sym", "t3d_sldae_a1_sym", "t1d_bdg_sym"]
 
 
 def _compare(name, nwf, nsteps, nmeas, tol=TOL, hkf=None):
@@ -108,7 +108,8 @@ def test_selfstart(has_gpu, name, nwf, nsteps, nmeas):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,nwf,nsteps,nmeas", [("t2d_slda", 24, 3, 2), ("t1d_aslda", 24, 3, 2), ("c4_bdg2d", 16, 4, 1),
-                                                   ("t3d_aslda", 24, 3, 2), ("t2d_vext", 24, 3, 1)])
+                                                   ("t3d_aslda", 24, 3, 2), ("t2d_vext", 24, 3, 1),
+                                                   ("t2d_aslda_sym", 24, 3, 2), ("t1d_bdg_sym", 24, 3, 2)])
 def test_quantum_friction(has_gpu, name, nwf, nsteps, nmeas):
     """steps with quantum friction switched on over the run (ramp included): friction
     densities, particle control and the friction-modified H (pca_kernels.cu:497-539)"""

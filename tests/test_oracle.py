@@ -7,7 +7,8 @@ import pytest
 from oracle_lib import Oracle
 from parity_util import inputs
 
-SMALL = ["t1d_custom", "t1d_aslda", "t2d_slda", "t2d_bdg", "t3d_slda", "t3d_aslda", "t2d_sldae", "t1d_sldae_a1"]
+SMALL = ["t1d_custom", "t1d_aslda", "t2d_slda", "t2d_bdg", "t3d_slda", "t3d_aslda", "t2d_sldae", "t1d_sldae_a1",
+         "t2d_aslda_sym", "t1d_bdg_sym"]
 
 
 @pytest.mark.parametrize("name", SMALL + ["c1_bdg1d", "c2_slda2d", "c4_bdg2d"])

@@ -190,9 +190,6 @@
 #define CURRENT_CORRECTIONS
 #undef FAST_CONST_EFFECTIVE_MASS_MODE
 #endif
-#ifdef SPINSYMMETRY_MODE
-#error "SPINSYMMETRY_MODE is not provided by this library"
-#endif
 
 #if REGULARIZATION_SCHEME==CUBIC_CUTOFF
 #define USE_CUBIC_CUTOFF

@@ -1604,7 +1604,7 @@ extern "C" int wtd_adjoint(wtd_ctx *c, int it0, int nsteps, int checkpoint_every
     if (!c || !loss || nsteps < 1 || checkpoint_every < 0 || nparam < 0 || nparam > MAX_USER_PARAMS ||
         (grad && nparam < 1))
         return WTD_ERR_ARG;
-#if defined(WTD_ADJOINT_CONTACT_BDG) && defined(FAST_CONST_EFFECTIVE_MASS_MODE)
+#if defined(WTD_ADJOINT_CONTACT_BDG) && defined(FAST_CONST_EFFECTIVE_MASS_MODE) && !defined(SPINSYMMETRY_MODE)
     if (c->prec != WTD_FP64 || c->staged || c->sstride != 12 * WTD_NUMEL) return WTD_ERR_UNSUPPORTED;
     WTD_CU(cudaSetDevice(c->dev));
     const int r = adjoint_run(c, it0, nsteps, checkpoint_every, mask, nparam, loss, grad);

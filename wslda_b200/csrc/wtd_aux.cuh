@@ -23,8 +23,29 @@ __global__ void wtd_dens_reduce(const double *slots, int nslots, double *dens, i
     int q = (i < 2 * N) ? 0 : 1 + (i - 2 * N) / N; /* 0: nu, 1: rho_a, 2: tau_a, ..., 6: rho_b ... */
     bool needed = full || q == 0 || q == 1 || q == 6 || i >= 12 * N;
     double s = 0.0;
+#ifdef SPINSYMMETRY_MODE
+    /* spin-symmetric system (pca_dens.cu:55-124, 365-461; symmetrize_densities_device): both
+     * spin channels take the sum of the u (f) and v (1 - f) contributions, nu and the friction
+     * pairing density D count twice.  The sum is linear, so it is taken here, over the slots,
+     * before the exchange between ranks. */
+    if (needed) {
+        size_t j = (size_t)i;
+        double mul = 1.0;
+        if (q == 0 || i >= 14 * N) mul = 2.0, j = (size_t)-1;
+        else if (i >= 13 * N) j = (size_t)i - N;                /* U_b <- U_a + U_b */
+        else if (i >= 12 * N) j = (size_t)i + N;                /* U_a <- U_a + U_b */
+        else if (q >= 6) j = (size_t)i - 5 * (size_t)N;          /* b <- a + b */
+        else j = (size_t)i + 5 * (size_t)N;                      /* a <- a + b */
+        if (j == (size_t)-1)
+            for (int k = 0; k < nslots; k++) s += slots[(size_t)k * stride + i];
+        else
+            for (int k = 0; k < nslots; k++) s += slots[(size_t)k * stride + i] + slots[(size_t)k * stride + j];
+        s *= mul;
+    }
+#else
     if (needed)
         for (int k = 0; k < nslots; k++) s += slots[(size_t)k * stride + i];
+#endif
     dens[i] = s * inv_lperp;
 }
 

@@ -317,6 +317,10 @@ __global__ void k_qf_dens_compat(int n, const double2 *wf, const double2 *lap, c
         dre += ((v.x * lu.x + v.y * lu.y) + (lv.x * u.x + lv.y * u.y)) * (fm - f) * wc;
         dim += ((v.x * lu.y - v.y * lu.x) + (lv.x * u.y - lv.y * u.x)) * (fm - f) * wc;
     }
+#ifdef SPINSYMMETRY_MODE
+    /* spin-symmetric system (pca_dens.cu:411-420): U_a = U_b = both sums, D counted twice */
+    ua += ub; ub = ua; dre *= 2.0; dim *= 2.0;
+#endif
     out[p] = ua * inv_lperp;
     out[N + p] = ub * inv_lperp;
     out[2 * (size_t)N + 2 * p] = -0.5 * dre * inv_lperp;
