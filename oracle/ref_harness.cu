@@ -91,6 +91,15 @@ extern "C" int refh_nhist(void) { return nhist_of_scheme(); }
  * quasiparticle energies (nwf), history slots f1..fq in the reference's order after the last
  * pointer rotation (q x 2*nwf*N complex), and the device time per step in ms.
  */
+/* energy log: when set, the 11 energy items after the initial measurement and after every
+ * measurement block ((nmeas + 1) x 11 doubles), as pca.c:970 and 1581 compute them */
+static double *elog = NULL;
+extern "C" int refh_set_energy_log(double *buf)
+{
+    elog = buf;
+    return 0;
+}
+
 /* Taylor self-start of the history (pca.c:1086-1330), off unless set */
 static int selfstart_on = 0;
 extern "C" int taylor_expansion_contribution(int it, double dt, int n, Z *hpsi, Z *upd, Z *contr, int nthreads);
@@ -336,6 +345,10 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
         CK(compute_potentials(it, d_dens, d_pots, 1.0, nthreads));
     }
 
+    if (elog) {
+        CK(compute_energy(it, d_dens, d_pots, d_work, nthreads));
+        CK(cudaMemcpy(elog, d_work, 11 * sizeof(double), cudaMemcpyDeviceToHost));
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0); cudaEventCreate(&e1);
     CK(cudaDeviceSynchronize());
@@ -385,6 +398,10 @@ extern "C" int refh_run(int nwf, const double *y0, const double *pots0, const do
             if (qfsw > 0.0) pcc = host_pccoeff();
             CK(HAPPLY(it + 1, d_f[0]));
             it++;
+        }
+        if (elog) {
+            CK(compute_energy(it, d_dens, d_pots, d_work, nthreads));
+            CK(cudaMemcpy(elog + 11 * (size_t)(im + 1), d_work, 11 * sizeof(double), cudaMemcpyDeviceToHost));
         }
     }
     cudaEventRecord(e1);

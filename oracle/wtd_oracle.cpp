@@ -1047,6 +1047,12 @@ int orc_codedim(void) { return CODEDIM; }
 int orc_nhist(void) { return NHIST; }
 int orc_dims(int *d) { d[0] = AXN[0]; d[1] = AXN[1]; d[2] = AXN[2]; return 0; }
 int orc_functional(void) { return FUNCTIONAL; }
+/* the user's host hook process_params (pca.c:903), as the reference's driver calls it */
+int orc_process_params(double *params, double *kF, double *mu)
+{
+    process_params(params, kF, mu, 0, NULL);
+    return 0;
+}
 int orc_const_mass(void)
 {
 #ifdef FAST_CONST_EFFECTIVE_MASS_MODE

@@ -63,6 +63,7 @@ class Oracle:
         L.orc_qf_densities.argtypes = [_dp]
         L.orc_subset_densities.argtypes = [_dp, _dp]
         L.orc_filter_field.argtypes = [_dp]
+        L.orc_process_params.argtypes = [_dp, _dp, _dp]
         self._xfn = None
         # the library is shared by every instance in the process: start from a plain run
         L.orc_set_high_k_filter(0, 0.0, 1.0)
@@ -87,6 +88,10 @@ class Oracle:
         cnt_p = None if cnt is None else np.ascontiguousarray(cnt, dtype=np.int32).ctypes.data_as(_ip)
         self.lib.orc_setup(self.S, _p(st), _p(np.ascontiguousarray(pots, dtype=np.float64)),
                            _p(np.ascontiguousarray(occ, dtype=np.float64)), _p(kky), _p(kkz), cnt_p, it0)
+
+    def process_params(self, params, kF, mu):
+        """the project's process_params hook on (params, kF[1], mu[2]) in place"""
+        self.lib.orc_process_params(_p(params), _p(kF), _p(mu))
 
     def initial_measurement(self):
         return self.lib.orc_initial_measurement()

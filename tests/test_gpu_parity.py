@@ -47,6 +47,14 @@ def test_c1_bdg1d_full_config(has_gpu):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["t3d_aslda", "t2d_sldae"])
+def test_variable_mass_many_states(has_gpu, name):
+    """variable effective mass with several states per CTA and padded rows: every operator of
+    the H application reads its transform before the next one overwrites the buffer"""
+    _compare(name, nwf=700, nsteps=3, nmeas=2)
+
+
+@pytest.mark.gpu
 def test_c2_slda2d_small_s(has_gpu):
     _compare("c2_slda2d", nwf=32, nsteps=3, nmeas=1)
 

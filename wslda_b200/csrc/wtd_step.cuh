@@ -283,6 +283,9 @@ __device__ __forceinline__ double hpsi_var(const TY *yu, const TY *yv, typename 
                 }
                 H[o] = h;
             }
+            /* every thread has read W (by point) before the next operator overwrites it (by
+             * padded index, another thread's points) */
+            __syncthreads();
         }
         /* - (1/4) lap(alpha psi) with the spin's sign */
         __syncthreads();
