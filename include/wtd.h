@@ -55,6 +55,7 @@ typedef struct wtd_ctx wtd_ctx;
 #define WTD_ERR_STATE -4
 #define WTD_ERR_NOMEM -5
 #define WTD_ERR_COMM -7   /* density exchange failed (NCCL missing or a collective error) */
+#define WTD_ERR_IO -8     /* checkpoint file missing, short or not writable */
 
 /* lattice and build facts of this library: dims[3], numel, codedim, scheme history length,
  * functional id (111 SLDA, 112 ASLDA, 113 BDG, 114 CUSTOMEDF), const-mass flag */
@@ -110,6 +111,31 @@ int wtd_download_qpe(wtd_ctx *ctx, double *host_qpe);
  * subset tracking (pca.c:842-870, 1056-1066) with weights[n] = 1 for the tracked states, 0
  * otherwise (any real weights are accepted).  FP64. */
 int wtd_subset_densities(wtd_ctx *ctx, const double *weights, double *host_dens);
+
+/* Checkpoints in the reference's file layout (hpc-engine/tdwslda_checkpoint.c; restart with
+ * inittype 5, pca.c:781-830): <dir>/checkpoint_<rank / howmany>, one file per IO group of
+ * `howmany` ranks (MPI_NP_PER_IO_GROUP).  Every rank of a run calls save / load with its own
+ * context, whose state count must be the rank's share of info.nwf (getnwfip,
+ * pca_utils.c:660). */
+typedef struct {
+    double t0;                        /* time of the state */
+    double mu_a, mu_b, ec, kF, eF, Effg, beta;
+    int nwf;                          /* states of all ranks */
+} wtd_checkpoint_info;
+/* the file header (load_nwf, tdwslda_checkpoint.c:26-66) */
+int wtd_checkpoint_info_read(const char *dir, int rank, int howmany, wtd_checkpoint_info *info);
+/* write this rank's part (save_checkpoint, :215-364): E_n (ctx S values), k_perp (2D: k_z;
+ * 1D: S k_y then S k_z; NULL in 3D), the states, the ABM history and, from the first rank of
+ * a group, the header and the potentials */
+int wtd_checkpoint_save(wtd_ctx *ctx, const char *dir, int rank, int nranks, int howmany,
+                        const wtd_checkpoint_info *info, const double *En, const double *kperp);
+/* read this rank's part back (load_checkpoint, :69-212): states, history, potentials, the
+ * occupations fbeta(E_n, beta) and k_perp (1D: cnt = the degeneracy counts the run started
+ * with, which the file does not hold); then the restart's measurement (densities, history
+ * kept).  Set the constants first (t0 = info.t0 from wtd_checkpoint_info_read).  The outputs
+ * may be NULL. */
+int wtd_checkpoint_load(wtd_ctx *ctx, const char *dir, int rank, int nranks, int howmany, const int *cnt,
+                        wtd_checkpoint_info *info, double *En, double *kperp);
 
 /* device pointers (for callers that keep data on the GPU): states, densities, potentials */
 int wtd_device_pointers(wtd_ctx *ctx, void **states, double **dens, double **pots);

@@ -41,6 +41,11 @@ SIGNATURES = {
     "wtd_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "wtd_selfstart": (ctypes.c_int, [ctypes.c_void_p]),
     "wtd_subset_densities": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    "wtd_checkpoint_info_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "wtd_checkpoint_save": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_void_p, _dp, _dp]),
+    "wtd_checkpoint_load": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           _ip, ctypes.c_void_p, _dp, _dp]),
     "wtd_energy": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "wtd_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "wtd_time_index": (ctypes.c_int, [ctypes.c_void_p]),
@@ -63,6 +68,16 @@ SIGNATURES = {
 }
 
 # host hook of a state-sharded run: int fn(void *user, double *dens, size_t count, void *stream)
+class CheckpointInfo(ctypes.Structure):
+    """wtd_checkpoint_info (include/wtd.h): the checkpoint file header"""
+    _fields_ = [("t0", ctypes.c_double), ("mu_a", ctypes.c_double), ("mu_b", ctypes.c_double),
+                ("ec", ctypes.c_double), ("kF", ctypes.c_double), ("eF", ctypes.c_double),
+                ("Effg", ctypes.c_double), ("beta", ctypes.c_double), ("nwf", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
 
 
@@ -90,6 +105,18 @@ def _p(a):
 
 class WtdError(RuntimeError):
     pass
+
+
+def checkpoint_info(project, directory, rank=0, howmany=24):
+    """the header of a checkpoint in the reference's layout (t0, mu, ec, kF, eF, Effg, beta,
+    nwf) as a dict"""
+    name = project.name if isinstance(project, Project) else project
+    lib = load_library(name)
+    ci = CheckpointInfo()
+    rc = lib.wtd_checkpoint_info_read(os.fsencode(directory), int(rank), int(howmany), ctypes.byref(ci))
+    if rc != 0:
+        raise WtdError(f"{name}: {lib.wtd_error_string(rc).decode()} ({rc})")
+    return ci.as_dict()
 
 
 class TDRun:
@@ -253,6 +280,26 @@ class TDRun:
     def adjoint_release(self):
         """free the adjoint's device workspace (kept between gradient calls)"""
         self._check(self.lib.wtd_adjoint_release(self.h))
+
+    def checkpoint_save(self, directory, info, En, kperp=None, rank=0, nranks=1, howmany=24):
+        """write this rank's part of <directory>/checkpoint_<rank // howmany> in the reference's
+        layout; info: dict of CheckpointInfo fields (nwf = states of all ranks)"""
+        ci = CheckpointInfo(**info)
+        en = np.ascontiguousarray(En, dtype=np.float64)
+        kp = None if kperp is None else np.ascontiguousarray(kperp, dtype=np.float64)
+        self._check(self.lib.wtd_checkpoint_save(self.h, os.fsencode(directory), int(rank), int(nranks), int(howmany),
+                                                 ctypes.byref(ci), _p(en), _p(kp)))
+
+    def checkpoint_load(self, directory, rank=0, nranks=1, howmany=24, cnt=None):
+        """read this rank's part back and measure; returns (info dict, E_n, k_perp)"""
+        ci = CheckpointInfo()
+        en = np.zeros(self.nwf)
+        kp = np.zeros(2 * self.nwf)
+        c = None if cnt is None else np.ascontiguousarray(cnt, dtype=np.int32)
+        self._check(self.lib.wtd_checkpoint_load(self.h, os.fsencode(directory), int(rank), int(nranks), int(howmany),
+                                                 None if c is None else c.ctypes.data_as(_ip), ctypes.byref(ci),
+                                                 _p(en), _p(kp)))
+        return ci.as_dict(), en, kp
 
     def set_params(self, params):
         self._params = np.ascontiguousarray(params, dtype=np.float64)

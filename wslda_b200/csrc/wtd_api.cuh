@@ -593,6 +593,7 @@ const char *wtd_error_string(int code)
     case WTD_ERR_NOMEM: return "out of device memory";
     case WTD_ERR_COMM: return "density exchange failed (NCCL not loadable, or a collective or hook error)";
     case -6: return "lattice too large for the fixed scratch of calculate_densities_noalloc (12*N doubles > 1 Mi words)";
+    case WTD_ERR_IO: return "checkpoint file missing, short or not writable";
     default: return "unknown error";
     }
 }

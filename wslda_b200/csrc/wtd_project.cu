@@ -19,3 +19,4 @@
 #define WTD_CODEDIM CODEDIM
 #include "wtd_compat.cuh"
 #include "wtd_api.cuh"
+#include "wtd_checkpoint.cuh"
