@@ -318,6 +318,14 @@ __device__ __forceinline__ double ld_keep(const double *a, uint64_t pol)
     asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
     return v;
 }
+/* read-only load with the same L2 policy, not volatile: for arrays that no thread writes while
+ * the kernel runs, so the compiler may schedule and batch these loads freely */
+__device__ __forceinline__ double ld_ro_keep(const double *a, uint64_t pol)
+{
+    double v;
+    asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
 __device__ __forceinline__ void st_keep(double *a, double v, uint64_t pol)
 {
     asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");

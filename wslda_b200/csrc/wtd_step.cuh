@@ -186,6 +186,7 @@ __device__ __forceinline__ double hpsi_const(const TY *yu, const TY *yv, typenam
     __syncthreads();
     fft_inverse<G, 2>(BU, (int)(BV - BU), tw);
     double q = 0.0;
+#pragma unroll 2
     for (int p = threadIdx.x; p < N; p += blockDim.x) {
         int o = G::off(p);
         TC ur, ui, vr, vi;
@@ -193,9 +194,9 @@ __device__ __forceinline__ double hpsi_const(const TY *yu, const TY *yv, typenam
             double2 u = to_d(yu[p]), v = to_d(yv[p]);
             ur = (TC)u.x; ui = (TC)u.y; vr = (TC)v.x; vi = (TC)v.y;
         }
-        const TC va = (TC)ld_keep(cf + CF_VA * N + p, pol), vb = (TC)ld_keep(cf + CF_VB * N + p, pol);
-        const TC dr = (TC)ld_keep(cf + CF_DRE * N + p, pol), di = (TC)ld_keep(cf + CF_DIM * N + p, pol);
-        const TC aa = (TC)ld_keep(cf + CF_AA * N + p, pol), ab = (TC)ld_keep(cf + CF_AB * N + p, pol);
+        const TC va = (TC)ld_ro_keep(cf + CF_VA * N + p, pol), vb = (TC)ld_ro_keep(cf + CF_VB * N + p, pol);
+        const TC dr = (TC)ld_ro_keep(cf + CF_DRE * N + p, pol), di = (TC)ld_ro_keep(cf + CF_DIM * N + p, pol);
+        const TC aa = (TC)ld_ro_keep(cf + CF_AA * N + p, pol), ab = (TC)ld_ro_keep(cf + CF_AB * N + p, pol);
         const TC ja = -aa * (TC)kp2, jb = -ab * (TC)kp2;
         C lu = BU[o], lv = BV[o];
         /* u' = (Va-mu_a+ja) u + D v + aa lap u ;  v' = -(Vb-mu_b+jb) v + D* u - ab lap v */
@@ -332,6 +333,30 @@ __device__ __forceinline__ void dens_limited(double *ds, int p, int N, double2 u
     st_keep(a1, s1 + (u.y * v.x - u.x * v.y) * fn, pol);
     st_keep(a2, s2 + (u.x * u.x + u.y * u.y) * fa, pol);
     st_keep(a3, s3 + (v.x * v.x + v.y * v.y) * fb, pol);
+}
+
+/* the same for two points at once (q valid when hq): all slot loads are issued before any
+ * store, so the two points share one L2 round trip (the loads and stores carry cache hints as
+ * volatile asm, which keeps them in program order) */
+__device__ __forceinline__ void dens_limited2(double *ds, int p, int q, bool hq, int N, double2 u, double2 v,
+                                              double2 u1, double2 v1, double f, double w, uint64_t pol)
+{
+    double fa = f * w, fb = (1.0 - f) * w, fn = (1.0 - 2.0 * f) * 0.5 * w;
+    double *a0 = ds + 2 * p, *a1 = ds + 2 * p + 1, *a2 = ds + 2 * (size_t)N + p, *a3 = ds + 7 * (size_t)N + p;
+    double *b0 = ds + 2 * q, *b1 = ds + 2 * q + 1, *b2 = ds + 2 * (size_t)N + q, *b3 = ds + 7 * (size_t)N + q;
+    double s0 = ld_keep(a0, pol), s1 = ld_keep(a1, pol), s2 = ld_keep(a2, pol), s3 = ld_keep(a3, pol);
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    if (hq) { t0 = ld_keep(b0, pol); t1 = ld_keep(b1, pol); t2 = ld_keep(b2, pol); t3 = ld_keep(b3, pol); }
+    st_keep(a0, s0 + (u.x * v.x + u.y * v.y) * fn, pol);
+    st_keep(a1, s1 + (u.y * v.x - u.x * v.y) * fn, pol);
+    st_keep(a2, s2 + (u.x * u.x + u.y * u.y) * fa, pol);
+    st_keep(a3, s3 + (v.x * v.x + v.y * v.y) * fb, pol);
+    if (hq) {
+        st_keep(b0, t0 + (u1.x * v1.x + u1.y * v1.y) * fn, pol);
+        st_keep(b1, t1 + (u1.y * v1.x - u1.x * v1.y) * fn, pol);
+        st_keep(b2, t2 + (u1.x * u1.x + u1.y * u1.y) * fa, pol);
+        st_keep(b3, t3 + (v1.x * v1.x + v1.y * v1.y) * fb, pol);
+    }
 }
 
 /* tau and j contributions of one normalised component (pca_dens.cu:41-108).  B0 holds the
@@ -489,6 +514,7 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
         TH *__restrict__ fk_out = (TH *)a.slot[NH - 1];
         TH *__restrict__ p_out = (TH *)a.slot[NH - 2];
         double nrm = 0.0;
+#pragma unroll 2
         for (int p = threadIdx.x; p < N; p += blockDim.x) {
             const int o = G::off(p);
             /* all global loads of this point first (both components), then arithmetic */
@@ -554,20 +580,30 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
         if (a.nrm_out && threadIdx.x == 0) a.nrm_out[n] = nrm_tot;
         /* ---- normalise, store, densities ---- */
         const double f = a.occ[n], w = a.wcnt[n];
-        for (int p = threadIdx.x; p < N; p += blockDim.x) {
-            const int o = G::off(p);
-            C hu = HU[o], hv = HV[o];
-            double2 u = make_double2((double)hu.x * c, (double)hu.y * c);
-            double2 v = make_double2((double)hv.x * c, (double)hv.y * c);
-            TY su = from_d<TY>(u), sv = from_d<TY>(v);
-            st_stream(ou + p, su); st_stream(ov + p, sv);
-            u = to_d(su); v = to_d(sv);
-            dens_limited(ds, p, N, u, v, f, w, pol);
-            if (GRAD) {
-                C cu, cv;
-                cu.x = (TC)u.x; cu.y = (TC)u.y; cv.x = (TC)v.x; cv.y = (TC)v.y;
-                HU[o] = cu; HV[o] = cv;
+        for (int p = threadIdx.x; p < N; p += 2 * blockDim.x) {
+            /* two points per iteration (p, q = p + blockDim.x) so that their density-slot
+             * updates share one L2 round trip */
+            const int q = p + blockDim.x;
+            const bool hq = q < N;
+            double2 uu[2], vv[2];
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                if (k == 1 && !hq) { uu[1] = vv[1] = make_double2(0.0, 0.0); break; }
+                const int pp = k ? q : p, o = G::off(pp);
+                C hu = HU[o], hv = HV[o];
+                double2 u = make_double2((double)hu.x * c, (double)hu.y * c);
+                double2 v = make_double2((double)hv.x * c, (double)hv.y * c);
+                TY su = from_d<TY>(u), sv = from_d<TY>(v);
+                st_stream(ou + pp, su); st_stream(ov + pp, sv);
+                u = to_d(su); v = to_d(sv);
+                uu[k] = u; vv[k] = v;
+                if (GRAD) {
+                    C cu, cv;
+                    cu.x = (TC)u.x; cu.y = (TC)u.y; cv.x = (TC)v.x; cv.y = (TC)v.y;
+                    HU[o] = cu; HV[o] = cv;
+                }
             }
+            dens_limited2(ds, p, q, hq, N, uu[0], vv[0], uu[1], vv[1], f, w, pol);
         }
         if (GRAD) {
             /* const mass: (HU, HV) = (BU, BV) hold the state, B2 is work.
