@@ -152,6 +152,7 @@ int taylor_expansion_contribution(int it, double dt, int n, wtd_z *wf_hpsi, wtd_
 /* external fields to host arrays (hpc-engine/pca_kernels.cu:1110-1181) */
 int get_v_ext(int datadim, int spin, int it, double *data);
 int get_delta_ext(int datadim, int it, void *deltain, void *data);
+int get_velocity_ext(int datadim, int spin, int it, double *data);
 
 #ifdef __cplusplus
 }

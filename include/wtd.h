@@ -137,6 +137,16 @@ int wtd_checkpoint_save(wtd_ctx *ctx, const char *dir, int rank, int nranks, int
 int wtd_checkpoint_load(wtd_ctx *ctx, const char *dir, int rank, int nranks, int howmany, const int *cnt,
                         wtd_checkpoint_info *info, double *En, double *kperp);
 
+/* Measurements in the W-data format of the reference's TD codes (wslda_writevars.c, lib/wdata):
+ * <prefix>.wtxt plus <prefix>_<var>.wdat per variable.  vars: the input file's writevar tags
+ * (rho, j, tau, V, V_ext, velocity_ext, delta, delta_ext, nu, alpha, A), separated by spaces or
+ * commas; NULL or "" gives the reference's default "rho delta j".  dt_cycle: the time between
+ * cycles (timesteps * dt); float_prec: 1 writes f32 (writeprec f).  begin removes the set's
+ * old .wdat files; each write appends one cycle of the current densities and potentials at the
+ * context's time index and rewrites the metadata. */
+int wtd_wdata_begin(wtd_ctx *ctx, const char *prefix, const char *vars, double t0, double dt_cycle, int float_prec);
+int wtd_wdata_write(wtd_ctx *ctx);
+
 /* device pointers (for callers that keep data on the GPU): states, densities, potentials */
 int wtd_device_pointers(wtd_ctx *ctx, void **states, double **dens, double **pots);
 /* CUDA stream the context orders its work on (cudaStream_t) */

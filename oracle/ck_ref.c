@@ -30,57 +30,8 @@
 #define CK_N NXYZ
 #endif
 
-int shim_rank = 0, shim_size = 1, shim_howmany = 1;
 /* the process id that the reference's drivers keep globally (pca.c:39) */
 int wsldapid = 0;
-
-int MPI_Comm_size(MPI_Comm comm, int *size)
-{
-    if (comm == MPI_COMM_WORLD) { *size = shim_size; return 0; }
-    int g = comm - 1, first = g * shim_howmany;
-    *size = (shim_size - first < shim_howmany) ? shim_size - first : shim_howmany;
-    return 0;
-}
-int MPI_Comm_rank(MPI_Comm comm, int *rank)
-{
-    *rank = (comm == MPI_COMM_WORLD) ? shim_rank : shim_rank - (comm - 1) * shim_howmany;
-    return 0;
-}
-int MPI_Comm_split(MPI_Comm comm, int color, int key, MPI_Comm *newcomm)
-{
-    (void)comm; (void)key;
-    *newcomm = color + 1;
-    return 0;
-}
-int MPI_File_open(MPI_Comm comm, const char *name, int amode, MPI_Info info, MPI_File *fh)
-{
-    (void)comm; (void)info;
-    int fl = (amode & MPI_MODE_WRONLY) ? O_WRONLY : O_RDONLY;
-    if (amode & MPI_MODE_CREATE) fl |= O_CREAT;
-    int fd = open(name, fl, 0644);
-    if (fd < 0) { *fh = NULL; return 1; }
-    *fh = (MPI_File)malloc(sizeof(**fh));
-    (*fh)->fd = fd;
-    return 0;
-}
-int MPI_File_close(MPI_File *fh)
-{
-    if (*fh) { close((*fh)->fd); free(*fh); *fh = NULL; }
-    return 0;
-}
-int MPI_File_read_at(MPI_File fh, MPI_Offset off, void *buf, int count, MPI_Datatype type, MPI_Status *st)
-{
-    ssize_t r = pread(fh->fd, buf, (size_t)count * type, (off_t)off);
-    if (st) st->count = (int)(r / type);
-    return r == (ssize_t)((size_t)count * type) ? 0 : 1;
-}
-int MPI_File_write_at(MPI_File fh, MPI_Offset off, const void *buf, int count, MPI_Datatype type, MPI_Status *st)
-{
-    ssize_t r = pwrite(fh->fd, buf, (size_t)count * type, (off_t)off);
-    if (st) st->count = (int)(r / type);
-    return r == (ssize_t)((size_t)count * type) ? 0 : 1;
-}
-int MPI_Abort(MPI_Comm comm, int code) { (void)comm; exit(code); }
 
 /* the reference's host/device copies, on host memory */
 int memcopy_host2gpu(void *host, void *gpu, size_t size) { memcpy(gpu, host, size); return 0; }

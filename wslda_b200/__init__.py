@@ -41,6 +41,9 @@ SIGNATURES = {
     "wtd_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "wtd_selfstart": (ctypes.c_int, [ctypes.c_void_p]),
     "wtd_subset_densities": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    "wtd_wdata_begin": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_int]),
+    "wtd_wdata_write": (ctypes.c_int, [ctypes.c_void_p]),
     "wtd_checkpoint_info_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "wtd_checkpoint_save": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_void_p, _dp, _dp]),
@@ -300,6 +303,16 @@ class TDRun:
                                                  None if c is None else c.ctypes.data_as(_ip), ctypes.byref(ci),
                                                  _p(en), _p(kp)))
         return ci.as_dict(), en, kp
+
+    def wdata_begin(self, prefix, vars=None, t0=0.0, dt_cycle=1.0, float_prec=False):
+        """start a W-data set <prefix>.wtxt / <prefix>_<var>.wdat (the reference's output format)"""
+        v = None if vars is None else (vars if isinstance(vars, str) else " ".join(vars)).encode()
+        self._check(self.lib.wtd_wdata_begin(self.h, os.fsencode(prefix), v, float(t0), float(dt_cycle),
+                                             1 if float_prec else 0))
+
+    def wdata_write(self):
+        """append one cycle of the current densities and potentials"""
+        self._check(self.lib.wtd_wdata_write(self.h))
 
     def set_params(self, params):
         self._params = np.ascontiguousarray(params, dtype=np.float64)

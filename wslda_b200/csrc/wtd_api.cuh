@@ -50,6 +50,9 @@ struct wtd_ctx {
     void *xuser;
     /* adjoint workspace kept between gradient calls (AdjWork, released with the context) */
     void *adj;
+    /* W-data output set (wtd_wdata.cuh) and its destructor */
+    void *wdata;
+    void (*wdata_free)(void *);
     /* high-k filter of the effective masses after every functional evaluation (variable mass) */
     int hkf_mode;
     double hkf_mu, hkf_T;
@@ -696,6 +699,7 @@ int wtd_destroy(wtd_ctx *c)
     cudaSetDevice(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
     adj_release(c);
+    if (c->wdata && c->wdata_free) c->wdata_free(c->wdata);
     if (c->nccl && nccl_api()) nccl_api()->comm_destroy((ncclComm_t)c->nccl);
     if (c->timing)
         for (int p = 0; p < 2; p++)

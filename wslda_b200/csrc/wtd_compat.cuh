@@ -349,6 +349,18 @@ __global__ void k_get_dext(int it, const Complex *din, Complex *out)
     out[i] = WTD_D_EXT(ix, iy, iz, it, din[i]);
 }
 
+/* the external velocity field, x, y, z blocks of N */
+__global__ void k_get_velext(int it, int spin, double *out)
+{
+    int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i >= WTD_NUMEL) return;
+    int ix, iy, iz; wtd_decode(i, ix, iy, iz);
+    /* the user's hook, whether or not the field acts (pca_kernels.cu:1149-1160) */
+    out[i] = velocity_ext(ix, iy, iz, it, spin, XAXIS, dc_params, dc_extra_data_size, dc_extra_data);
+    out[WTD_NUMEL + i] = velocity_ext(ix, iy, iz, it, spin, YAXIS, dc_params, dc_extra_data_size, dc_extra_data);
+    out[2 * WTD_NUMEL + i] = velocity_ext(ix, iy, iz, it, spin, ZAXIS, dc_params, dc_extra_data_size, dc_extra_data);
+}
+
 static __device__ double g_sum_tmp[1 << 16];   /* outputs of k_sum_many before they are moved */
 
 /* the spectral tables every compatibility call uses (built once per process) */
@@ -1000,6 +1012,16 @@ int get_v_ext(int datadim, int spin, int it, double *data)
     if (cudaMalloc((void **)&t, sizeof(double) * WTD_NUMEL) != cudaSuccess) return 1;
     k_get_vext<<<(WTD_NUMEL + 127) / 128, 128>>>(it, spin, t);
     int r = cudaMemcpy(data, t, sizeof(double) * WTD_NUMEL, cudaMemcpyDeviceToHost) != cudaSuccess;
+    cudaFree(t);
+    return r;
+}
+/* velocity_ext on the lattice, x, y, z blocks into data (3 N host doubles; wslda_writevars.c:80) */
+int get_velocity_ext(int datadim, int spin, int it, double *data)
+{
+    double *t = NULL;
+    if (cudaMalloc((void **)&t, sizeof(double) * 3 * WTD_NUMEL) != cudaSuccess) return 1;
+    k_get_velext<<<(WTD_NUMEL + 127) / 128, 128>>>(it, spin, t);
+    int r = cudaMemcpy(data, t, sizeof(double) * 3 * WTD_NUMEL, cudaMemcpyDeviceToHost) != cudaSuccess;
     cudaFree(t);
     return r;
 }

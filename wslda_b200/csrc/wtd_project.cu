@@ -20,3 +20,4 @@
 #include "wtd_compat.cuh"
 #include "wtd_api.cuh"
 #include "wtd_checkpoint.cuh"
+#include "wtd_wdata.cuh"
