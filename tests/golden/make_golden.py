@@ -78,6 +78,8 @@ QF_CASES = {
     "t3d_aslda": (24, 3, 2, True),
     "t2d_aslda_sym": (24, 3, 2, True),
     "t1d_bdg_sym": (24, 3, 2, True),
+    "c3_aslda3d": (8, 2, 1, False),
+    "t2d_big": (8, 3, 1, False),
 }
 QF_PARAMS = (0.5, 0.3, 0.2, 10.0, 0.0, 100.0, 0.02)
 

@@ -117,10 +117,12 @@ def test_selfstart(has_gpu, name, nwf, nsteps, nmeas):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,nwf,nsteps,nmeas", [("t2d_slda", 24, 3, 2), ("t1d_aslda", 24, 3, 2), ("c4_bdg2d", 16, 4, 1),
                                                    ("t3d_aslda", 24, 3, 2), ("t2d_vext", 24, 3, 1),
-                                                   ("t2d_aslda_sym", 24, 3, 2), ("t1d_bdg_sym", 24, 3, 2)])
+                                                   ("t2d_aslda_sym", 24, 3, 2), ("t1d_bdg_sym", 24, 3, 2),
+                                                   ("c3_aslda3d", 8, 2, 1), ("t2d_big", 8, 3, 1)])
 def test_quantum_friction(has_gpu, name, nwf, nsteps, nmeas):
     """steps with quantum friction switched on over the run (ramp included): friction
-    densities, particle control and the friction-modified H (pca_kernels.cu:497-539)"""
+    densities, particle control and the friction-modified H (pca_kernels.cu:497-539), on the
+    fused lattices and on the plane/pencil path (c3_aslda3d, t2d_big)"""
     import sys, os
     sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
     from golden.make_golden import QF_PARAMS

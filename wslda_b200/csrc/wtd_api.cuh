@@ -305,28 +305,13 @@ static int functional(wtd_ctx *c, int it)
     return WTD_OK;
 }
 
-/* densities from the slots, tau, potentials and H coefficients at time index it */
-static int after_pass(wtd_ctx *c, bool full, int it)
+/* the effective-mass filter, then the H coefficients from the potentials at time index it:
+ * filtered in place, or, while quantum friction acts, from the friction-modified fields */
+static int coef_with_friction(wtd_ctx *c, int it)
 {
     constexpr int N = WTD_NUMEL;
-    const bool qf = c->qfsw > 0.0;
-    const int words = (qf ? 16 : 12) * N;
-    wtd_dens_reduce<<<(words + 255) / 256, 256, 0, c->st>>>(c->dslot, c->grid, c->dens, N, full ? 1 : 0, 1.0 / WTD_LPERP,
-                                                            (size_t)c->sstride, words);
-    WTD_LAUNCHED(c);
-    WTD_TRY(exchange(c, c->dens, (size_t)words));
-    if (full) {
-        constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
-        if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
-        static bool attr = false;
-        if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_tau_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
-        wtd_tau_kernel<WG><<<2, 512, sm, c->st>>>(c->dens, c->tw, c->ktab);
-        WTD_LAUNCHED(c);
-    }
-    if (it < 0) return WTD_OK;
-    WTD_TRY(functional(c, it));
     WTD_TRY(filter_alpha(c));
-    if (!qf) {
+    if (!(c->qfsw > 0.0)) {
         WTD_TRY(filter_h(c));
         return coef_from_pots(c, it);
     }
@@ -348,6 +333,29 @@ static int after_pass(wtd_ctx *c, bool full, int it)
     WTD_CU(cudaMemcpyAsync(c->pots, c->qfld, 4 * (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
 #endif
     return WTD_OK;
+}
+
+/* densities from the slots, tau, potentials and H coefficients at time index it */
+static int after_pass(wtd_ctx *c, bool full, int it)
+{
+    constexpr int N = WTD_NUMEL;
+    const bool qf = c->qfsw > 0.0;
+    const int words = (qf ? 16 : 12) * N;
+    wtd_dens_reduce<<<(words + 255) / 256, 256, 0, c->st>>>(c->dslot, c->grid, c->dens, N, full ? 1 : 0, 1.0 / WTD_LPERP,
+                                                            (size_t)c->sstride, words);
+    WTD_LAUNCHED(c);
+    WTD_TRY(exchange(c, c->dens, (size_t)words));
+    if (full) {
+        constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
+        if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+        static bool attr = false;
+        if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_tau_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+        wtd_tau_kernel<WG><<<2, 512, sm, c->st>>>(c->dens, c->tw, c->ktab);
+        WTD_LAUNCHED(c);
+    }
+    if (it < 0) return WTD_OK;
+    WTD_TRY(functional(c, it));
+    return coef_with_friction(c, it);
 }
 
 /* the friction switch at time t (pca_utils.c:779-790, 1055-1060): 0 when every coefficient is
@@ -379,7 +387,14 @@ static int staged_densities(wtd_ctx *c, bool grads)
     WTD_LAUNCHED(c);
     wtd_dens_reduce<<<(12 * N + 255) / 256, 256, 0, c->st>>>(c->dslot, G, c->dens, N, grads ? 1 : 0, 1.0 / WTD_LPERP);
     WTD_LAUNCHED(c);
-    WTD_TRY(exchange(c, c->dens, 12 * (size_t)N));
+    const bool qf = c->qfsw > 0.0;
+    if (qf) {
+        /* the friction densities U_a, U_b, D after the 12 N words (pca.c:1426-1429) */
+        k_qf_dens_compat<<<(N + 255) / 256, 256, 0, c->st>>>(S, (const double2 *)c->y, c->dlap, c->occ, NULL, c->kp2,
+                                                            c->wcnt, c->dens + 12 * (size_t)N, 1.0 / WTD_LPERP);
+        WTD_LAUNCHED(c);
+    }
+    WTD_TRY(exchange(c, c->dens, (qf ? 16 : 12) * (size_t)N));
     if (grads) WTD_TRY(big_tau(c->dens, c->stage3d, c->tw, c->ktab, c->st));
     return WTD_OK;
 }
@@ -397,17 +412,10 @@ static int staged_potentials(wtd_ctx *c, int it)
     wslda_density D = convert_into_wslda_density(c->dens, N);
     wslda_potential P = convert_into_wslda_potential(c->pots, N, NULL);
     int pb = (N + 127) / 128;
-    wtd_potentials_kernel<<<pb, 128, 0, c->st>>>(it, D, P, 1.0);
-    WTD_LAUNCHED(c);
-#ifdef ENABLE_MODIFY_POTENTIALS
-    modify_potentials<<<pb, 128, 0, c->st>>>(it, D, P);
-    WTD_LAUNCHED(c);
-#endif
-    WTD_TRY(filter_fields(c));
-    wtd_prep_coef<<<pb, 128, 0, c->st>>>(it, P, c->cf);
-    WTD_LAUNCHED(c);
+    (void)D; (void)pb;
+    WTD_TRY(functional(c, it));
+    WTD_TRY(coef_with_friction(c, it));
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
-    WTD_TRY(big_prep_var(c->cf, c->stage3d, c->tw, c->ktab, c->st));
     /* lap(alpha psi) for the variable-mass kinetic term (pca.c:1455-1456) */
     size_t M = (size_t)2 * c->S * N;
     k_mul_alpha<<<(unsigned)((M + 255) / 256), 256, 0, c->st>>>(c->S, (const double2 *)c->y, c->dalap, P.alpha_a, P.alpha_b);
@@ -444,6 +452,10 @@ static int staged_step(wtd_ctx *c, bool last)
     double2 *f[5] = {NULL, NULL, NULL, NULL, NULL};
     for (int sl = 0; sl < NH; sl++) f[sl] = (double2 *)c->hist[(c->head + (sl == 0 ? NH - 1 : sl - 1)) % NH];
     const bool var = WTD_VAR;
+    /* the friction switch of this step (pca.c:1405); while it acts every half step takes the
+     * gradient path (pca.c:1412-1414, 1483-1485) */
+    c->qfsw = qf_switch(c, hc_t0 + (c->it + 1) * c->dt);
+    const bool qf = c->qfsw > 0.0;
     /* predictor (pca.c:1407-1465) */
     if (NH == 3) k_abm_step1<3><<<nb, 256, 0, c->st>>>(M, (double2 *)c->y, f[0], f[1], f[2], NULL, NULL, c->dt);
     else if (NH == 4) k_abm_step1<4><<<nb, 256, 0, c->st>>>(M, (double2 *)c->y, f[0], f[1], f[2], f[3], NULL, c->dt);
@@ -451,8 +463,8 @@ static int staged_step(wtd_ctx *c, bool last)
     WTD_LAUNCHED(c);
     k_normalize<<<c->S, 256, 0, c->st>>>(c->S, (double2 *)c->y);
     WTD_LAUNCHED(c);
-    WTD_TRY(staged_derivs(c, var));
-    WTD_TRY(staged_densities(c, var));
+    WTD_TRY(staged_derivs(c, var || qf));
+    WTD_TRY(staged_densities(c, var || qf));
     WTD_TRY(staged_potentials(c, c->it + 1));
     WTD_TRY(staged_hamiltonian(c, c->dlap));
     /* corrector (pca.c:1469-1566) */
@@ -461,7 +473,7 @@ static int staged_step(wtd_ctx *c, bool last)
     WTD_LAUNCHED(c);
     k_normalize<<<c->S, 256, 0, c->st>>>(c->S, (double2 *)c->y);
     WTD_LAUNCHED(c);
-    const bool g = var || last;
+    const bool g = var || last || qf;
     WTD_TRY(staged_derivs(c, g));
     WTD_TRY(staged_densities(c, g));
     WTD_TRY(staged_potentials(c, c->it + 1));
@@ -1040,7 +1052,7 @@ int wtd_set_quantum_friction(wtd_ctx *c, double alpha, double beta, double gamma
 {
     if (!c) return WTD_ERR_ARG;
     const bool on = alpha != 0.0 || beta != 0.0 || gamma != 0.0;
-    if (on && (c->staged || !(ramp > 0.0))) return c->staged ? WTD_ERR_UNSUPPORTED : WTD_ERR_ARG;
+    if (on && !(ramp > 0.0)) return WTD_ERR_ARG;
     c->qf[0] = alpha; c->qf[1] = beta; c->qf[2] = gamma; c->qf[3] = nreq;
     c->qf[4] = start; c->qf[5] = stop; c->qf[6] = ramp;
     c->sstride = (on ? 16 : 12) * WTD_NUMEL;
