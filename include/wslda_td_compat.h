@@ -110,7 +110,8 @@ int calculate_quantum_friction_densities(int n, wtd_z *wf, wtd_z *d_wf_laplace, 
  * scratch is a fixed 8 MiB device array inside the library, so it accepts lattices with
  * 12*N doubles <= 1 Mi words (N <= 87381 points) and returns WTD_ERR_NOALLOC_SIZE (-6)
  * otherwise.  The array is shared by all calls: calls that overlap on the GPU race on it.
- * The first call on a device resolves the array's device address with that device current. */
+ * The first call on a device resolves the array's device address with that device current;
+ * make that first call before any stream capture on the device. */
 #if WTD_CODEDIM == 3
 int calculate_densities_noalloc(int n, wtd_z *wf, wtd_z *wf_d_dx, wtd_z *wf_d_dy, wtd_z *wf_d_dz, wtd_z *d_wf_laplace,
                                 double *d_fbetaEn, double *weights, double *d_densities, int gradients_computed, int nthreads);

@@ -482,6 +482,8 @@ static int compat_planewave(int n, const double *kky, const double *kkz, const i
  * work is issued.  The number of CTAs is min(2 per SM, n, 8 MiB / (12*N*8)).
  * Every call shares the array and leaves its partial sums in it; each call clears the part it
  * uses first.  Calls that overlap on the GPU (other host threads, other streams) race on it.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress); make
+ * it before any stream capture on that device.
  * -------------------------------------------------------------------------------------*/
 #define WTD_NOALLOC_BYTES (8u << 20)
 static __device__ __align__(256) double wtd_noalloc_scratch[WTD_NOALLOC_BYTES / sizeof(double)];
