@@ -55,6 +55,31 @@ def test_variable_mass_many_states(has_gpu, name):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name,nwf,prec,tol", [("t2d_slda", 24, 1, 1e-5), ("t2d_slda", 24, 2, 1e-5), ("t3d_aslda", 24, 1, 1e-5),
+                                                ("c3_aslda3d", 8, 1, 1e-6), ("t2d_big", 8, 1, 1e-6)])
+def test_mixed_forms_track_fp64(has_gpu, name, nwf, prec, tol):
+    """the FP32-mixed forms (complex64 states; FP64 or complex64 history) against the FP64
+    oracle over a measurement block: the fused lattices compute FFT and H psi in FP32, the
+    plane/pencil lattices (c3_aslda3d, t2d_big) keep FP64 arithmetic and round the states to
+    complex64 after each renormalisation"""
+    o = run_oracle(name, nwf, 3, 1)
+    g = run_gpu(name, nwf, 3, 1, precision=prec)
+    n = o["densities"].size // 12
+    errs = density_errors(g["densities"], o["densities"], n)
+    for k in ("rho_a", "rho_b", "nu"):
+        assert errs[k] < tol, (name, prec, k, errs[k])
+    e_o, e_g = o["energy"][:7].sum(), g["energy"][:7].sum()
+    assert abs(e_g - e_o) / abs(e_o) < tol
+
+
+@pytest.mark.gpu
+def test_mixed_h32_refused_on_plane_pencil_path(has_gpu):
+    from wslda_b200 import TDRun, WtdError
+    with pytest.raises(WtdError):
+        TDRun("c3_aslda3d", 8, precision=2)
+
+
+@pytest.mark.gpu
 def test_c2_slda2d_small_s(has_gpu):
     _compare("c2_slda2d", nwf=32, nsteps=3, nmeas=1)
 

@@ -377,12 +377,34 @@ static double qf_switch(const wtd_ctx *c, double t)
  * derivatives (wtd_fft3d.cuh), CTA-per-state renormalisation and H psi with <H> subtraction,
  * slot-accumulated densities, the ABM update as one elementwise kernel per half step.
  * -------------------------------------------------------------------------------------*/
+/* the plane/pencil path computes in FP64.  In the mixed form (WTD_MIXED_H64) the states
+ * stay complex64 between calls and the step works on an FP64 copy in c->stage, rounded to
+ * complex64 where the fused form stores the states: after each renormalisation */
+static double2 *st_y(wtd_ctx *c) { return c->prec == WTD_FP64 ? (double2 *)c->y : c->stage; }
+static int st_load(wtd_ctx *c)
+{
+    if (c->prec == WTD_FP64) return WTD_OK;
+    const size_t n2 = (size_t)2 * c->S * WTD_NUMEL;
+    wtd_convert_out<float2><<<(unsigned)((n2 + 255) / 256), 256, 0, c->st>>>((const float2 *)c->y, c->stage, n2);
+    WTD_LAUNCHED(c);
+    return WTD_OK;
+}
+/* store the FP64 copy as the complex64 states and continue from the stored values */
+static int st_round(wtd_ctx *c)
+{
+    if (c->prec == WTD_FP64) return WTD_OK;
+    const size_t n2 = (size_t)2 * c->S * WTD_NUMEL;
+    wtd_convert_in<float2><<<(unsigned)((n2 + 255) / 256), 256, 0, c->st>>>(c->stage, (float2 *)c->y, n2);
+    WTD_LAUNCHED(c);
+    return st_load(c);
+}
+
 static int staged_densities(wtd_ctx *c, bool grads)
 {
     constexpr int N = WTD_NUMEL;
     const int S = c->S;
     int G = c->grid;
-    k_dens_compat<<<G, 256, 0, c->st>>>(S, (const double2 *)c->y, c->ddx, c->ddy, c->ddz, c->dlap, c->occ, NULL, c->kp2,
+    k_dens_compat<<<G, 256, 0, c->st>>>(S, st_y(c), c->ddx, c->ddy, c->ddz, c->dlap, c->occ, NULL, c->kp2,
                                         c->wcnt, c->dslot, grads ? 1 : 0);
     WTD_LAUNCHED(c);
     wtd_dens_reduce<<<(12 * N + 255) / 256, 256, 0, c->st>>>(c->dslot, G, c->dens, N, grads ? 1 : 0, 1.0 / WTD_LPERP);
@@ -390,7 +412,7 @@ static int staged_densities(wtd_ctx *c, bool grads)
     const bool qf = c->qfsw > 0.0;
     if (qf) {
         /* the friction densities U_a, U_b, D after the 12 N words (pca.c:1426-1429) */
-        k_qf_dens_compat<<<(N + 255) / 256, 256, 0, c->st>>>(S, (const double2 *)c->y, c->dlap, c->occ, NULL, c->kp2,
+        k_qf_dens_compat<<<(N + 255) / 256, 256, 0, c->st>>>(S, st_y(c), c->dlap, c->occ, NULL, c->kp2,
                                                             c->wcnt, c->dens + 12 * (size_t)N, 1.0 / WTD_LPERP);
         WTD_LAUNCHED(c);
     }
@@ -402,8 +424,8 @@ static int staged_densities(wtd_ctx *c, bool grads)
 static int staged_derivs(wtd_ctx *c, bool grads)
 {
     const int nf = 2 * c->S;
-    if (grads) return big_derivs((double2 *)c->y, nf, c->dlap, c->ddx, c->ddy, CODEDIM >= 3 ? c->ddz : NULL, c->tw, c->ktab, c->st);
-    return big_derivs((double2 *)c->y, nf, c->dlap, NULL, NULL, NULL, c->tw, c->ktab, c->st);
+    if (grads) return big_derivs(st_y(c), nf, c->dlap, c->ddx, c->ddy, CODEDIM >= 3 ? c->ddz : NULL, c->tw, c->ktab, c->st);
+    return big_derivs(st_y(c), nf, c->dlap, NULL, NULL, NULL, c->tw, c->ktab, c->st);
 }
 
 static int staged_potentials(wtd_ctx *c, int it)
@@ -418,7 +440,7 @@ static int staged_potentials(wtd_ctx *c, int it)
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
     /* lap(alpha psi) for the variable-mass kinetic term (pca.c:1455-1456) */
     size_t M = (size_t)2 * c->S * N;
-    k_mul_alpha<<<(unsigned)((M + 255) / 256), 256, 0, c->st>>>(c->S, (const double2 *)c->y, c->dalap, P.alpha_a, P.alpha_b);
+    k_mul_alpha<<<(unsigned)((M + 255) / 256), 256, 0, c->st>>>(c->S, st_y(c), c->dalap, P.alpha_a, P.alpha_b);
     WTD_LAUNCHED(c);
     WTD_TRY(big_derivs(c->dalap, 2 * c->S, c->dalap, NULL, NULL, NULL, c->tw, c->ktab, c->st));
 #endif
@@ -428,7 +450,7 @@ static int staged_potentials(wtd_ctx *c, int it)
 
 static int staged_hamiltonian(wtd_ctx *c, double2 *out)
 {
-    k_hamiltonian_compat<<<c->S, 256, 0, c->st>>>(c->S, (const double2 *)c->y, out, c->ddx, c->ddy, c->ddz, c->dlap,
+    k_hamiltonian_compat<<<c->S, 256, 0, c->st>>>(c->S, st_y(c), out, c->ddx, c->ddy, c->ddz, c->dlap,
                                                   c->dalap, c->cf, c->kp2, c->qpe, NULL);
     WTD_LAUNCHED(c);
     return WTD_OK;
@@ -436,8 +458,10 @@ static int staged_hamiltonian(wtd_ctx *c, double2 *out)
 
 static int staged_initial(wtd_ctx *c)
 {
-    k_normalize<<<c->S, 256, 0, c->st>>>(c->S, (double2 *)c->y);
+    WTD_TRY(st_load(c));
+    k_normalize<<<c->S, 256, 0, c->st>>>(c->S, st_y(c));
     WTD_LAUNCHED(c);
+    WTD_TRY(st_round(c));
     WTD_TRY(staged_derivs(c, true));
     return staged_densities(c, true);
 }
@@ -457,22 +481,26 @@ static int staged_step(wtd_ctx *c, bool last)
     c->qfsw = qf_switch(c, hc_t0 + (c->it + 1) * c->dt);
     const bool qf = c->qfsw > 0.0;
     /* predictor (pca.c:1407-1465) */
-    if (NH == 3) k_abm_step1<3><<<nb, 256, 0, c->st>>>(M, (double2 *)c->y, f[0], f[1], f[2], NULL, NULL, c->dt);
-    else if (NH == 4) k_abm_step1<4><<<nb, 256, 0, c->st>>>(M, (double2 *)c->y, f[0], f[1], f[2], f[3], NULL, c->dt);
-    else k_abm_step1<5><<<nb, 256, 0, c->st>>>(M, (double2 *)c->y, f[0], f[1], f[2], f[3], f[4], c->dt);
+    WTD_TRY(st_load(c));
+    double2 *Y = st_y(c);
+    if (NH == 3) k_abm_step1<3><<<nb, 256, 0, c->st>>>(M, Y, f[0], f[1], f[2], NULL, NULL, c->dt);
+    else if (NH == 4) k_abm_step1<4><<<nb, 256, 0, c->st>>>(M, Y, f[0], f[1], f[2], f[3], NULL, c->dt);
+    else k_abm_step1<5><<<nb, 256, 0, c->st>>>(M, Y, f[0], f[1], f[2], f[3], f[4], c->dt);
     WTD_LAUNCHED(c);
-    k_normalize<<<c->S, 256, 0, c->st>>>(c->S, (double2 *)c->y);
+    k_normalize<<<c->S, 256, 0, c->st>>>(c->S, Y);
     WTD_LAUNCHED(c);
+    WTD_TRY(st_round(c));
     WTD_TRY(staged_derivs(c, var || qf));
     WTD_TRY(staged_densities(c, var || qf));
     WTD_TRY(staged_potentials(c, c->it + 1));
     WTD_TRY(staged_hamiltonian(c, c->dlap));
     /* corrector (pca.c:1469-1566) */
     const double cc = (NH == 3) ? 9. / 24. : 251. / 720.;
-    k_abm_step4<<<nb, 256, 0, c->st>>>(M, c->dlap, (double2 *)c->y, f[NH - 1], c->dt, cc);
+    k_abm_step4<<<nb, 256, 0, c->st>>>(M, c->dlap, Y, f[NH - 1], c->dt, cc);
     WTD_LAUNCHED(c);
-    k_normalize<<<c->S, 256, 0, c->st>>>(c->S, (double2 *)c->y);
+    k_normalize<<<c->S, 256, 0, c->st>>>(c->S, Y);
     WTD_LAUNCHED(c);
+    WTD_TRY(st_round(c));
     const bool g = var || last || qf;
     WTD_TRY(staged_derivs(c, g));
     WTD_TRY(staged_densities(c, g));
@@ -641,7 +669,8 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
         if (pf) c->prefetch = atoi(pf) & 3;
     }
     c->staged = WTD_BIG ? 1 : 0;
-    if (c->staged && precision != WTD_FP64) { free(c); return WTD_ERR_UNSUPPORTED; }
+    /* plane/pencil lattices: FP64, or complex64 states with FP64 history and arithmetic */
+    if (c->staged && precision == WTD_MIXED_H32) { free(c); return WTD_ERR_UNSUPPORTED; }
     int per_sm = c->staged ? 2 : occupancy_per_sm(c);
     c->grid = nsm * per_sm;
     if (c->grid > nwf) c->grid = nwf;
