@@ -666,7 +666,7 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     c->prefetch = 1;
     {
         const char *pf = getenv("WTD_PREFETCH");
-        if (pf) c->prefetch = atoi(pf) & 3;
+        if (pf) c->prefetch = atoi(pf) & 15;
     }
     c->staged = WTD_BIG ? 1 : 0;
     /* plane/pencil lattices: FP64, or complex64 states with FP64 history and arithmetic */

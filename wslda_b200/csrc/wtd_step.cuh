@@ -67,7 +67,8 @@ struct StepArgs {
     double dt;
     int S;
     int fk_given;       /* pass A: f_k is already in ring slot NH-1 */
-    int prefetch;       /* bit 0: next state's y, bit 1: this state's ABM history into L2 */
+    int prefetch;       /* bit 0: next state's y; bits 1-3: how many of this state's ABM history
+                         * arrays go into L2 ahead of the FFT phase (7: all) */
     int accumulate;     /* add to the density slot (otherwise start from zero) */
     int sstride;        /* density-slot words per CTA: 12 N, or 16 N with quantum friction */
     int qf;             /* accumulate the quantum-friction densities (needs GRAD) */
@@ -465,13 +466,14 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
          * state's y (used by the next iteration), so HBM streams while the SM computes */
         if (threadIdx.x == 0) {
             const size_t hb = (size_t)N * sizeof(TH), yb = (size_t)N * sizeof(TY);
-            if (!(a.prefetch & 2)) {
+            const int nh = (a.prefetch >> 1) & 7;
+            if (nh == 0) {
             } else if (PASS == 0) {
-                for (int j = 0; j < NH - 1; j++) {
+                for (int j = 0; j < NH - 1 && j < nh; j++) {
                     prefetch_l2((const TH *)a.slot[j] + (size_t)n * N, hb);
                     prefetch_l2((const TH *)a.slot[j] + SN + (size_t)n * N, hb);
                 }
-                if (!haveH) {
+                if (!haveH && nh >= NH) {
                     prefetch_l2((const TH *)a.slot[NH - 1] + (size_t)n * N, hb);
                     prefetch_l2((const TH *)a.slot[NH - 1] + SN + (size_t)n * N, hb);
                 }
