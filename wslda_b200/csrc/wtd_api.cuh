@@ -424,8 +424,11 @@ static int staged_densities(wtd_ctx *c, bool grads)
 static int staged_derivs(wtd_ctx *c, bool grads)
 {
     const int nf = 2 * c->S;
-    if (grads) return big_derivs(st_y(c), nf, c->dlap, c->ddx, c->ddy, CODEDIM >= 3 ? c->ddz : NULL, c->tw, c->ktab, c->st);
-    return big_derivs(st_y(c), nf, c->dlap, NULL, NULL, NULL, c->tw, c->ktab, c->st);
+    c->launches += 2;
+    if (grads)
+        return big_derivs_sep(st_y(c), nf, c->dlap, c->ddx, c->ddy, CODEDIM >= 3 ? c->ddz : NULL, NULL, NULL, c->tw,
+                              c->ktab, c->st);
+    return big_derivs_sep(st_y(c), nf, c->dlap, NULL, NULL, NULL, NULL, NULL, c->tw, c->ktab, c->st);
 }
 
 static int staged_potentials(wtd_ctx *c, int it)
@@ -438,11 +441,10 @@ static int staged_potentials(wtd_ctx *c, int it)
     WTD_TRY(functional(c, it));
     WTD_TRY(coef_with_friction(c, it));
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
-    /* lap(alpha psi) for the variable-mass kinetic term (pca.c:1455-1456) */
-    size_t M = (size_t)2 * c->S * N;
-    k_mul_alpha<<<(unsigned)((M + 255) / 256), 256, 0, c->st>>>(c->S, st_y(c), c->dalap, P.alpha_a, P.alpha_b);
-    WTD_LAUNCHED(c);
-    WTD_TRY(big_derivs(c->dalap, 2 * c->S, c->dalap, NULL, NULL, NULL, c->tw, c->ktab, c->st));
+    /* lap(alpha psi) for the variable-mass kinetic term (pca.c:1455-1456), the product with
+     * alpha taken as the fields are loaded */
+    WTD_TRY(big_derivs_sep(st_y(c), 2 * c->S, c->dalap, NULL, NULL, NULL, P.alpha_a, P.alpha_b, c->tw, c->ktab, c->st));
+    c->launches += 2;
 #endif
     c->have_coef = 1;
     return WTD_OK;
@@ -1125,7 +1127,7 @@ static int ss_derivs(wtd_ctx *c, SelfWork &w, const double2 *in, int grads)
 {
     const int nf = 2 * c->S;
     double2 *dx = grads ? w.ddx : NULL, *dy = (grads && CODEDIM >= 2) ? w.ddy : NULL, *dz = (grads && CODEDIM >= 3) ? w.ddz : NULL;
-    if (WTD_BIG) return big_derivs((double2 *)in, nf, w.dlap, dx, dy, dz, c->tw, c->ktab, c->st);
+    if (WTD_BIG) return big_derivs_sep(in, nf, w.dlap, dx, dy, dz, NULL, NULL, c->tw, c->ktab, c->st);
     if (k_derivs_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     static bool attr = false;
     if (!attr) { WTD_CU(cudaFuncSetAttribute(k_derivs<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k_derivs_smem)); attr = true; }
@@ -1160,9 +1162,11 @@ static int ss_alap(wtd_ctx *c, SelfWork &w, const double2 *in)
 #ifndef FAST_CONST_EFFECTIVE_MASS_MODE
     constexpr size_t N = WTD_NUMEL;
     const size_t M = (size_t)2 * c->S * N;
+    if (WTD_BIG)
+        return big_derivs_sep(in, 2 * c->S, w.dalap, NULL, NULL, NULL, c->pots + 4 * N, c->pots + 5 * N, c->tw, c->ktab,
+                              c->st);
     k_mul_alpha<<<(unsigned)((M + 255) / 256), 256, 0, c->st>>>(c->S, in, w.dalap, c->pots + 4 * N, c->pots + 5 * N);
     WTD_LAUNCHED(c);
-    if (WTD_BIG) return big_derivs(w.dalap, 2 * c->S, w.dalap, NULL, NULL, NULL, c->tw, c->ktab, c->st);
     k_derivs<WG><<<2 * c->S, 512, k_derivs_smem, c->st>>>(w.dalap, NULL, NULL, NULL, w.dalap, c->tw, c->ktab);
     WTD_LAUNCHED(c);
 #else

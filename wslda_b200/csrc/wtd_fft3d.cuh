@@ -137,6 +137,174 @@ static int big_derivs(double2 *in, int nf, double2 *lap, double2 *dx, double2 *d
     return cudaGetLastError() == cudaSuccess ? WTD_OK : WTD_ERR_CUDA;
 }
 
+/* ---------------------------------------------------------------------------------------
+ * Separable derivative sets of the state fields.  The multipliers of d/dy, d/dz and of the
+ * (y, z) part of the laplacian do not depend on k_x, and those of d/dx and of the x part do not
+ * depend on (k_y, k_z).  The transforms along the other axes therefore cancel:
+ *
+ *   d/dy f = IFFT_yz[i k_y FFT_yz f] / (NY NZ)          d/dx f = IFFT_x[i k_x FFT_x f] / NX
+ *   lap f  = IFFT_yz[-(k_y^2 + k_z^2) FFT_yz f] / (NY NZ) + IFFT_x[-k_x^2 FFT_x f] / NX
+ *
+ * with the reference's Nyquist zeroing of first derivatives (pca_derivative.cu:152-171).  Two
+ * passes, no transpose between CTAs:
+ *   k_sep_planes : one CTA per (field, x plane): d/dy, d/dz and the (y, z) part of lap;
+ *   k_sep_pencils: one CTA per (field, group of x pencils): d/dx, and lap += its x part.
+ * A full set costs 3 reads + 5 writes of the fields, a laplacian 3 reads + 2 writes, against
+ * 6 + 9 and 3 + 3 for big_derivs.  Optional point weights multiply field f by wa (f < nfa) or
+ * wb before the transforms: lap(alpha psi) of the variable-mass kinetic term
+ * (multiply_wf_by_alpha + compute_laplace, pca.c:1455-1456) in one go.
+ * The input must not alias an output.
+ * -------------------------------------------------------------------------------------*/
+#define WTD_SEP_NT 256
+/* pencils per CTA of the x pass: up to 32 (512-byte rows), at most 2048 points, dividing NY*NZ */
+#define WTD_PXS_CAP (2048 / (NX) >= 32 ? 32 : 2048 / (NX) >= 16 ? 16 : 2048 / (NX) >= 8 ? 8 : 4)
+#define WTD_PXS (WTD_NYZ % WTD_PXS_CAP == 0 ? WTD_PXS_CAP : WTD_PX)
+
+template <class GP>
+__global__ void __launch_bounds__(WTD_SEP_NT) k_sep_planes(const double2 *__restrict__ in, double2 *lap, double2 *dy,
+                                                          double2 *dz, const double *wa, const double *wb, int nfa,
+                                                          const double2 *gtw_yz, const double *gk)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *B = (double2 *)smem_raw;
+    double2 *W = B + GP::padded;
+    double2 *tw = W + GP::padded;
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + GP::twtotal);
+    constexpr int NP = GP::ntot;
+    for (int t = threadIdx.x; t < GP::N0 + GP::N1; t += WTD_SEP_NT) tw[t] = gtw_yz[t];
+    for (int t = threadIdx.x; t < 6 * WTD_KT; t += WTD_SEP_NT) kt[t / WTD_KT][t % WTD_KT] = gk[t];
+    const int f = blockIdx.x / NX, x = blockIdx.x - f * NX;
+    const size_t base = (size_t)blockIdx.x * NP;   /* planes of a field are contiguous */
+    const double *w = wa ? (f < nfa ? wa : wb) + (size_t)x * NP : nullptr;
+    for (int p = threadIdx.x; p < NP; p += WTD_SEP_NT) {
+        double2 z = in[base + p];
+        if (w) {
+            const double a = w[p];
+            z = make_double2(z.x * a, z.y * a);
+        }
+        B[GP::off(p)] = z;
+    }
+    __syncthreads();
+    fft_forward<GP, 1>(B, 0, tw);
+    const double inv = 1.0 / (double)NP;
+#pragma unroll
+    for (int op = 0; op < 3; op++) {
+        double2 *o = op == 0 ? dy : op == 1 ? dz : lap;
+        if (!o) continue;
+        double2 *T = (op == 2) ? B : W; /* the laplacian comes last and works in place */
+        for (int p = threadIdx.x; p < NP; p += WTD_SEP_NT) {
+            const int yq = p / NZ, zq = p - yq * NZ;
+            const double2 z = B[GP::off(p)];
+            double2 r;
+            if (op == 2) {
+                const double ky = kt[1][yq], kz = kt[2][zq];
+                const double sc = -(ky * ky + kz * kz) * inv;
+                r = make_double2(z.x * sc, z.y * sc);
+            } else {
+                const double k = (op == 0 ? kt[4][yq] : kt[5][zq]) * inv;
+                r = make_double2(-k * z.y, k * z.x);
+            }
+            T[GP::off(p)] = r;
+        }
+        __syncthreads();
+        fft_inverse<GP, 1>(T, 0, tw);
+        for (int p = threadIdx.x; p < NP; p += WTD_SEP_NT) o[base + p] = T[GP::off(p)];
+        __syncthreads();
+    }
+}
+
+template <class GX>
+__global__ void __launch_bounds__(WTD_SEP_NT) k_sep_pencils(const double2 *__restrict__ in, double2 *lap, double2 *dx,
+                                                           const double *wa, const double *wb, int nfa,
+                                                           const double2 *gtw_x, const double *gk)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *B = (double2 *)smem_raw;
+    double2 *W = B + GX::padded;
+    double2 *tw = W + GX::padded;
+    double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + GX::twtotal);
+    constexpr int NXL = GX::N0, PX = GX::N1, NYZ = NY * NZ, N = NX * NY * NZ, groups = NYZ / PX;
+    for (int t = threadIdx.x; t < NXL; t += WTD_SEP_NT) tw[t] = gtw_x[t];
+    for (int t = threadIdx.x; t < 6 * WTD_KT; t += WTD_SEP_NT) kt[t / WTD_KT][t % WTD_KT] = gk[t];
+    const int f = blockIdx.x / groups, g = blockIdx.x - f * groups;
+    const size_t fb = (size_t)f * N;
+    const int q0 = g * PX;
+    const double *w = wa ? (f < nfa ? wa : wb) : nullptr;
+    /* element (x, q) of the field sits at x*NYZ + q */
+    for (int i = threadIdx.x; i < NXL * PX; i += WTD_SEP_NT) {
+        const int x = i / PX, j = i - x * PX;
+        const size_t pt = (size_t)x * NYZ + q0 + j;
+        double2 z = in[fb + pt];
+        if (w) {
+            const double a = w[pt];
+            z = make_double2(z.x * a, z.y * a);
+        }
+        B[GX::off(i)] = z;
+    }
+    __syncthreads();
+    fft_axis_fwd<GX, 0, 0, NXL, 1>(B, 0, tw);
+    const double inv = 1.0 / (double)NXL;
+    if (dx) {
+        for (int i = threadIdx.x; i < NXL * PX; i += WTD_SEP_NT) {
+            const int x = i / PX;
+            const double k = kt[3][x] * inv;
+            const double2 z = B[GX::off(i)];
+            W[GX::off(i)] = make_double2(-k * z.y, k * z.x);
+        }
+        __syncthreads();
+        fft_axis_inv<GX, 0, NXL, 1>(W, 0, tw);
+        for (int i = threadIdx.x; i < NXL * PX; i += WTD_SEP_NT) {
+            const int x = i / PX, j = i - x * PX;
+            dx[fb + (size_t)x * NYZ + q0 + j] = W[GX::off(i)];
+        }
+    }
+    if (lap) {
+        /* each thread scales the elements it reads: no barrier needed before the in-place write */
+        for (int i = threadIdx.x; i < NXL * PX; i += WTD_SEP_NT) {
+            const int x = i / PX;
+            const double kx = kt[0][x];
+            const double sc = -(kx * kx) * inv;
+            const double2 z = B[GX::off(i)];
+            B[GX::off(i)] = make_double2(z.x * sc, z.y * sc);
+        }
+        __syncthreads();
+        fft_axis_inv<GX, 0, NXL, 1>(B, 0, tw);
+        for (int i = threadIdx.x; i < NXL * PX; i += WTD_SEP_NT) {
+            const int x = i / PX, j = i - x * PX;
+            const size_t a = fb + (size_t)x * NYZ + q0 + j;
+            const double2 yz = lap[a], xp = B[GX::off(i)];
+            lap[a] = make_double2(yz.x + xp.x, yz.y + xp.y);
+        }
+    }
+}
+
+typedef Geo<NX, WTD_PXS, 1> WGXS;    /* WTD_PXS pencils along x */
+static constexpr size_t sep_planes_smem = 2 * (size_t)WGP::padded * sizeof(double2) + WGP::twtotal * sizeof(double2) + sizeof(KTab<WGP>);
+static constexpr size_t sep_pencils_smem = 2 * (size_t)WGXS::padded * sizeof(double2) + WGXS::twtotal * sizeof(double2) + sizeof(KTab<WGXS>);
+
+/* lap, d/dx, d/dy, d/dz (any may be NULL) of nf fields of N points; wa/wb: optional weights */
+static int big_derivs_sep(const double2 *in, int nf, double2 *lap, double2 *dx, double2 *dy, double2 *dz,
+                          const double *wa, const double *wb, const double2 *tw, const double *ktab, cudaStream_t st)
+{
+    constexpr int NYZ = NY * NZ;
+    if (NYZ % WTD_PXS != 0) return WTD_ERR_UNSUPPORTED;
+    if (sep_planes_smem > WTD_SMEM_MAX || sep_pencils_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
+    if (in == lap || in == dx || in == dy || in == dz) return WTD_ERR_ARG;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_sep_planes<WGP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sep_planes_smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_sep_pencils<WGXS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sep_pencils_smem) != cudaSuccess)
+            return WTD_ERR_CUDA;
+        attr = true;
+    }
+    const int nfa = nf / 2;
+    if (lap || dy || dz)
+        k_sep_planes<WGP><<<nf * NX, WTD_SEP_NT, sep_planes_smem, st>>>(in, lap, dy, dz, wa, wb, nfa, tw + NX, ktab);
+    if (lap || dx)
+        k_sep_pencils<WGXS><<<nf * (NYZ / WTD_PXS), WTD_SEP_NT, sep_pencils_smem, st>>>(in, lap, dx, wa, wb, nfa, tw, ktab);
+    return cudaGetLastError() == cudaSuccess ? WTD_OK : WTD_ERR_CUDA;
+}
+
 /* real field -> laplacian or d/dx_d of it (complex staging buffer of N points) */
 __global__ void k_real_to_c(const double *f, double2 *c, int n)
 {
