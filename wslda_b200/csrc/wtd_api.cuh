@@ -403,9 +403,18 @@ static int staged_densities(wtd_ctx *c, bool grads)
 {
     constexpr int N = WTD_NUMEL;
     const int S = c->S;
-    int G = c->grid;
-    k_dens_compat<<<G, 256, 0, c->st>>>(S, st_y(c), c->ddx, c->ddy, c->ddz, c->dlap, c->occ, NULL, c->kp2,
-                                        c->wcnt, c->dslot, grads ? 1 : 0);
+    /* parallel over points: WTD_DP_T-point tiles times state chunks, as many chunks as make one
+     * full wave of resident CTAs, at most one per slot of the context */
+    const int tiles = (N + WTD_DP_T - 1) / WTD_DP_T;
+    int nsm = 0, per_sm = 1;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dens_points, WTD_DP_T, 0);
+    int G = nsm * per_sm / tiles;
+    if (G > c->grid) G = c->grid;
+    if (G > S) G = S;
+    if (G < 1) G = 1;
+    k_dens_points<<<dim3(tiles, G), WTD_DP_T, 0, c->st>>>(S, G, st_y(c), c->ddx, c->ddy, c->ddz, c->dlap, c->occ,
+                                                          c->kp2, c->wcnt, c->dslot, grads ? 1 : 0);
     WTD_LAUNCHED(c);
     wtd_dens_reduce<<<(12 * N + 255) / 256, 256, 0, c->st>>>(c->dslot, G, c->dens, N, grads ? 1 : 0, 1.0 / WTD_LPERP);
     WTD_LAUNCHED(c);

@@ -180,6 +180,63 @@ __global__ void k_dens_compat(int n, const double2 *wf, const double2 *dx, const
     }
 }
 
+/* the same densities parallel over points, for lattices whose 12 N-word slot per CTA does not
+ * stay in L2 (3D 32^3: 3 MB per slot).  CTA (tile, chunk) sums the states of chunk
+ * [n*chunk/nchunk, n*(chunk+1)/nchunk) at WTD_DP_T points in registers, in state order, and
+ * writes the whole 12-block partial once into slot `chunk`; wtd_dens_reduce then sums the
+ * chunks in order (bitwise reproducible for a given nchunk). */
+#define WTD_DP_T 128
+__global__ void __launch_bounds__(WTD_DP_T) k_dens_points(int n, int nchunk, const double2 *__restrict__ wf,
+                                                          const double2 *__restrict__ dx, const double2 *__restrict__ dy,
+                                                          const double2 *__restrict__ dz, const double2 *__restrict__ lap,
+                                                          const double *__restrict__ fb, const double *__restrict__ kp2,
+                                                          const double *__restrict__ wcnt, double *slots, int grads)
+{
+    constexpr int N = WTD_NUMEL;
+    const int p = blockIdx.x * WTD_DP_T + threadIdx.x;
+    if (p >= N) return;
+    const int chunk = blockIdx.y;
+    const int s0 = (int)((long long)n * chunk / nchunk), s1 = (int)((long long)n * (chunk + 1) / nchunk);
+    const size_t SN = (size_t)n * N;
+    double nre = 0.0, nim = 0.0, ra = 0.0, rb = 0.0, ta = 0.0, tb = 0.0;
+    double ja[3] = {0.0, 0.0, 0.0}, jb[3] = {0.0, 0.0, 0.0};
+    const double2 *dd[3] = {dx, dy, dz};
+#pragma unroll 2
+    for (int s = s0; s < s1; s++) {
+        const double f = fb[s], w = wcnt[s], k2 = kp2[s];
+        const double fa = f * w, fbm = (1.0 - f) * w, fn = (1.0 - 2.0 * f) * 0.5 * w;
+        const size_t iu = (size_t)s * N + p, iv = SN + iu;
+        const double2 u = wf[iu], v = wf[iv];
+        nre += (u.x * v.x + u.y * v.y) * fn;
+        nim += (u.y * v.x - u.x * v.y) * fn;
+        ra += (u.x * u.x + u.y * u.y) * fa;
+        rb += (v.x * v.x + v.y * v.y) * fbm;
+        if (grads) {
+            const double2 lu = lap[iu], lv = lap[iv];
+            ta += (u.x * (lu.x - u.x * k2) + u.y * (lu.y - u.y * k2)) * fa;
+            tb += (v.x * (lv.x - v.x * k2) + v.y * (lv.y - v.y * k2)) * fbm;
+#pragma unroll
+            for (int d = 0; d < CODEDIM; d++) {
+                const double2 a = dd[d][iu], b = dd[d][iv];
+                ja[d] += (u.x * a.y - u.y * a.x) * fa;
+                jb[d] -= (v.x * b.y - v.y * b.x) * fbm;
+            }
+        }
+    }
+    double *ds = slots + (size_t)chunk * 12 * N;
+    ds[2 * p] = nre;
+    ds[2 * p + 1] = nim;
+    ds[2 * (size_t)N + p] = ra;
+    ds[3 * (size_t)N + p] = ta;
+    ds[7 * (size_t)N + p] = rb;
+    ds[8 * (size_t)N + p] = tb;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        ds[(4 + d) * (size_t)N + p] = ja[d];
+        ds[(9 + d) * (size_t)N + p] = jb[d];
+    }
+}
+
 /* apply_hamiltonian from caller-provided derivative arrays (pca_kernels.cu:233-495, 806-833):
  * one CTA per state; out may alias lap (each element is read before it is written) */
 __global__ void k_hamiltonian_compat(int n, const double2 *in, double2 *out, const double2 *dx, const double2 *dy,
