@@ -160,8 +160,10 @@ static int big_derivs(double2 *in, int nf, double2 *lap, double2 *dx, double2 *d
 #define WTD_PXS_CAP (2048 / (NX) >= 32 ? 32 : 2048 / (NX) >= 16 ? 16 : 2048 / (NX) >= 8 ? 8 : 4)
 #define WTD_PXS (WTD_NYZ % WTD_PXS_CAP == 0 ? WTD_PXS_CAP : WTD_PX)
 
+/* 4 CTAs per SM (at most 64 registers a thread): the plane FFT stages are latency-bound, and
+ * the register file otherwise admits 3 */
 template <class GP>
-__global__ void __launch_bounds__(WTD_SEP_NT) k_sep_planes(const double2 *__restrict__ in, double2 *lap, double2 *dy,
+__global__ void __launch_bounds__(WTD_SEP_NT, 4) k_sep_planes(const double2 *__restrict__ in, double2 *lap, double2 *dy,
                                                           double2 *dz, const double *wa, const double *wb, int nfa,
                                                           const double2 *gtw_yz, const double *gk)
 {
@@ -293,6 +295,8 @@ static int big_derivs_sep(const double2 *in, int nf, double2 *lap, double2 *dx, 
     static bool attr = false;
     if (!attr) {
         if (cudaFuncSetAttribute(k_sep_planes<WGP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sep_planes_smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_sep_planes<WGP>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
             cudaFuncSetAttribute(k_sep_pencils<WGXS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sep_pencils_smem) != cudaSuccess)
             return WTD_ERR_CUDA;
         attr = true;
