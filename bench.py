@@ -43,8 +43,8 @@ WORKLOADS = {
 
 
 # DRAM bytes (read + write) per state of the FP64 passes, from one ncu capture of the same
-# kernel on the same lattice (profiles/wtd_fused_pass_c2_slda2d_64x64.md: 1024 states, pass A
-# 1203 MB, pass B 437 MB); traffic per launch scales with the states processed
+# kernels on the same lattice (1024 states: pass A 1203 MB, pass B 437 MB of
+# dram__bytes_read.sum + dram__bytes_write.sum); traffic per launch scales with the states processed
 TRAFFIC_PER_STATE = {"c2_slda2d": {"pass_a": 1203152896 / 1024, "pass_b": 436638720 / 1024}}
 
 # bounded CPU samples of each workload (states, steps): about 10-30 s on the host cores
@@ -152,9 +152,67 @@ def pass_bytes(proj, precision):
     return a, b
 
 
+def total_energy(e):
+    """E_kin + E_pot + E_pair + E_curr + E_ext (V, Delta, v): the first 7 of the 11 energy items"""
+    return float(np.asarray(e)[:7].sum())
+
+
+def timed_blocks(r, stream, steps, blocks, dev, world):
+    """device time of `blocks` blocks of exactly `steps` steps each (CUDA events on the context
+    stream, barrier + synchronize around every block, max over ranks), clocks sampled during
+    all blocks; the pass times are accumulated over the blocks"""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms_blocks, launches = [], []
+    r.set_timing(True)
+    with ClockSampler(dev) as clk:
+        for _ in range(blocks):
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            l0 = r.launches()
+            e0.record(stream)
+            r.steps(steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            if world > 1:
+                t = torch.tensor([ms], device="cuda")
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                ms = float(t.item())
+            ms_blocks.append(ms)
+            launches.append(r.launches() - l0)
+    ta, tb, na, nb = r.pass_times()
+    r.set_timing(False)
+    return dict(ms_blocks=ms_blocks, ms=float(np.median(ms_blocks)), ms_a=ta / max(na, 1), ms_b=tb / max(nb, 1),
+                launches=int(np.median(launches)), clocks=clk.summary())
+
+
+def energy_drift(name, nwf, d, precision, steps, dev):
+    """|E(t) - E(0)| / |E(0)| over `steps` steps from the initial measurement, scaled to 1000
+    steps (time-independent fields conserve E); also returns the final densities"""
+    from wslda_b200 import TDRun
+    r = TDRun(name, nwf, precision=precision, device=dev)
+    r.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+    r.initial_measurement()
+    e0 = total_energy(r.energy())
+    r.steps(steps)
+    e1 = total_energy(r.energy())
+    dens = r.densities()
+    r.close()
+    return dict(steps=steps, e0=e0, e_t=e1, drift_per_1000_steps=abs(e1 - e0) / abs(e0) * 1000.0 / steps), dens
+
+
+def rho_err(dens, ref, n):
+    """relative L2 error of (rho_a, rho_b)"""
+    rho = np.concatenate([ref[2 * n:3 * n], ref[7 * n:8 * n]])
+    got = np.concatenate([dens[2 * n:3 * n], dens[7 * n:8 * n]])
+    return float(np.linalg.norm(got - rho) / np.linalg.norm(rho))
+
+
 def run_wtd(args, rank, world):
     import torch
-    from wslda_b200 import TDRun
+    from wslda_b200 import TDRun, WtdError
     wl = WORKLOADS[args.workload]
     name = wl["project"]
     nwf_total = args.nwf or wl["nwf"]
@@ -171,9 +229,12 @@ def run_wtd(args, rank, world):
     res = {}
     forms = [("fp64", 0)] + ([("mixed_h64", 1), ("mixed_h32", 2)] if not args.fp64_only else [])
     forms = [f for f in forms if f[0] in wl.get("forms", ("fp64", "mixed_h64", "mixed_h32"))]
-    base_precision = 0
     for label, prec in forms:
-        r = TDRun(name, nwf, precision=prec, device=dev)
+        try:
+            r = TDRun(name, nwf, precision=prec, device=dev)
+        except WtdError as ex:
+            res[label] = {"unsupported": str(ex)}
+            continue
         r.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
         if world > 1:
             from wslda_b200.sharding import attach_nccl
@@ -182,50 +243,35 @@ def run_wtd(args, rank, world):
         r.steps(args.warmup)
         r.sync()
         stream = torch.cuda.ExternalStream(r.stream())
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-        r.set_timing(True)
-        launches0 = r.launches()
-        with ClockSampler(dev) as clk:
-            e0.record(stream)
-            r.steps(args.steps)
-            e1.record(stream)
-            torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        ta, tb, na, nb = r.pass_times()
-        launches = r.launches() - launches0
-        t = torch.tensor([ms], device="cuda")
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-        dens = r.densities()
-        res[label] = dict(ms=ms, ms_a=ta / max(na, 1), ms_b=tb / max(nb, 1), launches=launches,
-                          clocks=clk.summary(), dens=dens, energy=r.energy(), prec=prec)
+        t = timed_blocks(r, stream, args.steps, args.blocks, dev, world)
+        t.update(dens=r.densities(), energy=r.energy(), prec=prec)
+        res[label] = t
         if label == "fp64":
             # e2e: public API with host buffers, pinned; H2D of the states and D2H of the densities
             # and energies are inside the timed region
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             hst = torch.from_numpy(d["states"].view(np.float64)).pin_memory()
             hd = torch.empty(12 * proj.numel, dtype=torch.float64).pin_memory()
-            r.set_timing(False)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            e0.record(stream)
-            r.lib.wtd_upload_states(r.h, hst.numpy().ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_double)))
-            r.initial_measurement()
-            r.steps(args.steps)
-            r.densities(out=hd.numpy())
-            en = r.energy()
-            e1.record(stream)
-            torch.cuda.synchronize()
-            e2e_ms = e0.elapsed_time(e1)
-            wall = (time.perf_counter() - t0) * 1e3
-            res["e2e"] = dict(ms=max(e2e_ms, 0.0), wall_ms=wall, h2d=hst.numel() * 8, d2h=hd.numel() * 8 + 11 * 8)
+            e2e_blocks = []
+            for _ in range(args.blocks):
+                torch.cuda.synchronize()
+                e0.record(stream)
+                r.lib.wtd_upload_states(r.h, hst.numpy().ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_double)))
+                r.initial_measurement()
+                r.steps(args.steps)
+                r.densities(out=hd.numpy())
+                r.energy()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                e2e_blocks.append(max(e0.elapsed_time(e1), 0.0))
+            res["e2e"] = dict(ms=float(np.median(e2e_blocks)), ms_blocks=e2e_blocks, h2d=hst.numel() * 8,
+                              d2h=hd.numel() * 8 + 11 * 8)
         if label == "fp64" and world == 1 and (args.adjoint or args.workload == "c4") and proj.cfg.get("stirrer_params"):
             res["adjoint"] = time_adjoint(r, proj, d, stream, args.adjoint_steps)
         r.close()
-    return proj, nwf, res
+        if world == 1 and args.drift_steps > 0 and wl.get("drift", False):
+            res[label]["drift"], res[label]["drift_dens"] = energy_drift(name, nwf, d, prec, args.drift_steps, dev)
+    return proj, nwf, d, res
 
 
 def time_adjoint(r, proj, d, stream, steps=0):
@@ -261,29 +307,137 @@ def time_adjoint(r, proj, d, stream, steps=0):
     out["grad_norm"] = float(np.linalg.norm(g))
     return out
 
-def reference_cuda(name, nwf, steps):
-    """The reference's own kernels (hpc-engine/*.cu built for sm_100a) on the same GPU."""
+def reference_cuda(name, nwf, steps, inp=None):
+    """The reference's own kernels (hpc-engine/*.cu built for sm_100a) on the same GPU and the same
+    inputs: initial measurement and one measurement block of `steps` steps (gradients on its last
+    step), as the reference driver runs them (pca.c:939-1586).  Returns the device time per step
+    and the block's densities and energies."""
     import ctypes
     so = os.path.join(REPO, "oracle", "_ref", name, "libref.so")
     if not os.path.exists(so):
         return None
-    from wslda_b200 import projects as P
-    proj, d = make_inputs(name, nwf)
+    proj, d = inp if inp is not None else make_inputs(name, nwf)
     lib = ctypes.CDLL(so, mode=ctypes.RTLD_LOCAL)
     dp = ctypes.POINTER(ctypes.c_double)
     lib.refh_run.argtypes = ([ctypes.c_int] + [dp] * 5 + [ctypes.POINTER(ctypes.c_int)] + [ctypes.c_double] * 7 +
                              [dp, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [dp] * 7)
     c = proj.constants()
     ms = np.zeros(1)
+    dens = np.zeros(12 * proj.numel)
+    energy = np.zeros(11)
     ex = np.ascontiguousarray(d["extra"])
     y = d["states"]
     rc = lib.refh_run(nwf, y.view(np.float64).ctypes.data_as(dp), d["pots"].ctypes.data_as(dp), d["occ"].ctypes.data_as(dp),
                       None, None, None, c["mu_a"], c["mu_b"], c["ec"], c["t0"], c["dt"], c["kF"], c["sclgth"],
                       np.ascontiguousarray(d["params"]).ctypes.data_as(dp), ex.ctypes.data if ex.size else None, ex.nbytes,
-                      steps, 1, 0, None, None, None, None, None, None, ms.ctypes.data_as(dp))
+                      steps, 1, 0, None, dens.ctypes.data_as(dp), None, energy.ctypes.data_as(dp), None, None,
+                      ms.ctypes.data_as(dp))
     if rc != 0:
         return {"error": f"refh_run rc={rc}"}
-    return {"ms_per_step": float(ms[0]), "value": nwf / (float(ms[0]) * 1e-3)}
+    return {"ms_per_step": float(ms[0]), "value": nwf / (float(ms[0]) * 1e-3), "steps": steps, "dens": dens,
+            "energy": energy}
+
+
+def parity_full_size(name, nwf, steps, dev, inp=None, ref=None):
+    """This library (FP64) against the reference's own kernels at the benchmarked state count:
+    the same seeded inputs, initial measurement and `steps` steps each; densities (relative L2
+    per block), the 11 energy items and the particle numbers.  The reference is the one-rank
+    restatement of pca.c:939-1586 over its unmodified kernels."""
+    from wslda_b200 import TDRun
+    from parity_util import density_errors
+    proj, d = inp if inp is not None else make_inputs(name, nwf)
+    if ref is None:
+        ref = reference_cuda(name, nwf, steps, (proj, d))
+    if not ref or "dens" not in ref:
+        return {"error": "reference kernels unavailable" if not ref else ref.get("error")}
+    r = TDRun(name, nwf, precision=0, device=dev)
+    r.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+    r.initial_measurement()
+    r.steps(steps)
+    dens, en = r.densities(), r.energy()
+    r.close()
+    derr = density_errors(dens, ref["dens"], proj.numel)
+    e_ref = ref["energy"]
+    eterm = {k: float(abs(en[i] - e_ref[i]) / max(abs(e_ref[i]), 1e-300))
+             for i, k in enumerate(["E_kin", "E_pot", "E_pair", "E_curr", "E_ext_V", "E_ext_delta", "E_ext_v",
+                                    "N_a", "N_b", "L_za", "L_zb"]) if abs(e_ref[i]) > 1e-12 * abs(e_ref[:7]).max()}
+    worst = max(max(derr.values()), max(eterm.values()))
+    return {"states": nwf, "steps": steps, "density_rel_l2": {k: float(v) for k, v in derr.items()},
+            "energy_rel": eterm, "worst": worst, "tolerance": 1e-10, "pass": bool(worst < 1e-10),
+            "against": "the reference's CUDA kernels (hpc-engine/*.cu, sm_100a) through oracle/ref_harness.cu, "
+                       "same GPU, same inputs"}
+
+
+def c3_comparison(args, dev):
+    """The 3D TD-ASLDA workload (32^3, 12,000 states, AB5AM5): FP64 against the FP32-mixed forms.
+    Each form is timed over `blocks` blocks of `c3_steps` steps at the full state count; its
+    density error against FP64 after those steps, and the energy drift of every form over
+    `c3_drift_steps` steps on a reduced state count (a smaller system of the same lattice and
+    functional, stated in the result)."""
+    import torch
+    from wslda_b200 import TDRun, WtdError
+    wl = WORKLOADS["c3"]
+    name, nwf = wl["project"], args.c3_nwf or wl["nwf"]
+    proj, d = make_inputs(name, nwf)
+    hbm, peak_kind = peaks()
+    out = {"workload": wl["desc"], "states": nwf, "steps": args.c3_steps, "blocks": args.blocks, "forms": {}}
+    dens64 = None
+    for label, prec in (("fp64", 0), ("mixed_h64", 1), ("mixed_h32", 2)):
+        try:
+            r = TDRun(name, nwf, precision=prec, device=dev)
+            r.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+            r.initial_measurement()
+            r.steps(args.warmup)
+            r.sync()
+        except WtdError as ex:
+            out["forms"][label] = {"unsupported": str(ex)}
+            try:
+                r.close()
+            except Exception:
+                pass
+            continue
+        stream = torch.cuda.ExternalStream(r.stream())
+        t = timed_blocks(r, stream, args.c3_steps, args.blocks, dev, 1)
+        dens = r.densities()
+        r.close()
+        ba, bb = pass_bytes(proj, prec)
+        f = {"value": nwf * args.c3_steps / (t["ms"] * 1e-3), "ms_per_step": t["ms"] / args.c3_steps,
+             "ms_blocks": t["ms_blocks"], "hbm_gbs_compulsory": (ba + bb) * nwf * args.c3_steps / (t["ms"] * 1e-3) / 1e9,
+             "launches_per_block": t["launches"], "clocks": t["clocks"]}
+        f["roofline_frac"] = f["hbm_gbs_compulsory"] / hbm
+        if label == "fp64":
+            dens64 = dens
+        else:
+            f["speedup_vs_fp64"] = out["forms"]["fp64"]["value"] and f["value"] / out["forms"]["fp64"]["value"]
+            f["density_rel_l2_err_vs_fp64"] = rho_err(dens, dens64, proj.numel)
+        out["forms"][label] = f
+        torch.cuda.empty_cache()
+    out["peak_gbs"] = hbm
+    out["peak_source"] = peak_kind
+    if args.c3_drift_steps > 0:
+        nd = args.c3_drift_nwf
+        pd, dd = make_inputs(name, nd)
+        drift = {"states": nd, "steps": args.c3_drift_steps}
+        d64 = None
+        for label, prec in (("fp64", 0), ("mixed_h64", 1), ("mixed_h32", 2)):
+            if "unsupported" in out["forms"].get(label, {}):
+                continue
+            res, dens = energy_drift(name, nd, dd, prec, args.c3_drift_steps, dev)
+            if label == "fp64":
+                d64 = dens
+            else:
+                res["density_rel_l2_err_vs_fp64"] = rho_err(dens, d64, pd.numel)
+            drift[label] = res
+        out["drift"] = drift
+    if args.c3_parity_nwf > 0 and not args.no_refcuda:
+        np_ = args.c3_parity_nwf
+        inp = make_inputs(name, np_)
+        ref = reference_cuda(name, np_, args.c3_parity_steps, inp)
+        out["parity_full_size"] = parity_full_size(name, np_, args.c3_parity_steps, dev, inp, ref)
+        if ref and "value" in ref:
+            out["reference_cuda"] = {"value": ref["value"], "ms_per_step": ref["ms_per_step"], "states": np_,
+                                     "steps": ref["steps"]}
+    return out
 
 
 def cpu_baseline(name, nwf_sample, steps, threads=None):
@@ -302,11 +456,29 @@ def cpu_baseline(name, nwf_sample, steps, threads=None):
             "sample": f"{nwf_sample} of the workload's states x {steps} steps, {dt:.1f} s, oracle/wtd_oracle.cpp"}
 
 
+def adjoint_c4(args, dev):
+    """Cost of the optimal-control gradient on the C4 workload (2D TD-BdG 48x48, 4608 states,
+    200 steps, checkpoints every 20): the gradient call over the loss-only forward"""
+    import torch
+    from wslda_b200 import TDRun
+    wl = WORKLOADS["c4"]
+    proj, d = make_inputs(wl["project"], wl["nwf"])
+    r = TDRun(wl["project"], wl["nwf"], precision=0, device=dev)
+    r.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+    stream = torch.cuda.ExternalStream(r.stream())
+    out = time_adjoint(r, proj, d, stream, args.adjoint_steps)
+    r.close()
+    out["workload"] = wl["desc"]
+    out["states"] = wl["nwf"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--blocks", type=int, default=3, help="timed blocks of --steps steps each; value is the median block")
     ap.add_argument("--impl", default="wtd", choices=["wtd", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--fp64-only", action="store_true")
@@ -315,8 +487,19 @@ def main():
     ap.add_argument("--no-refcuda", action="store_true")
     ap.add_argument("--adjoint", action="store_true", help="also time the adjoint gradient (stirrer projects)")
     ap.add_argument("--adjoint-steps", type=int, default=0, help="adjoint horizon (default: the project's steps)")
+    ap.add_argument("--drift-steps", type=int, default=1000, help="energy-drift run of every form (0: skip)")
+    ap.add_argument("--parity-steps", type=int, default=10, help="full-size parity against the reference kernels (0: skip)")
+    ap.add_argument("--extras", type=int, default=1, help="with the C2 workload at N=1: the C3 FP64-vs-mixed comparison "
+                    "and the C4 adjoint cost (0: skip)")
+    ap.add_argument("--c3-nwf", type=int, default=0)
+    ap.add_argument("--c3-steps", type=int, default=10)
+    ap.add_argument("--c3-drift-steps", type=int, default=1000)
+    ap.add_argument("--c3-drift-nwf", type=int, default=1024)
+    ap.add_argument("--c3-parity-nwf", type=int, default=4000)
+    ap.add_argument("--c3-parity-steps", type=int, default=10)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    args.blocks = max(args.blocks, 1)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     wl = WORKLOADS[args.workload]
@@ -329,8 +512,6 @@ def main():
             return
         sample = CPU_SAMPLE[args.workload]
         vals = []
-        for _ in range(args.warmup if False else 0):
-            pass
         cb = None
         t0 = time.perf_counter()
         for k in range(max(1, min(args.steps, 3))):
@@ -352,13 +533,17 @@ def main():
     if world > 1:
         import torch
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    proj, nwf, res = run_wtd(args, rank, world)
+    t_start = time.perf_counter()
+    wl["drift"] = args.workload == "c2"
+    proj, nwf, d, res = run_wtd(args, rank, world)
     nwf_total = args.nwf or wl["nwf"]
     if rank != 0:
         if world > 1:
             import torch
             torch.distributed.destroy_process_group()
         return
+    import torch
+    dev = torch.cuda.current_device()
     hbm, peak_kind = peaks()
     f = res["fp64"]
     value = nwf_total * args.steps / (f["ms"] * 1e-3)
@@ -369,6 +554,7 @@ def main():
     achieved = (ba * nwf / (f["ms_a"] * 1e-3) if fused else (ba + bb) * nwf * args.steps / (f["ms"] * 1e-3)) / 1e9
     line = {
         "metric": metric, "value": value, "unit": metric, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "blocks": args.blocks, "ms_blocks": f["ms_blocks"],
         "ms_per_step": f["ms"] / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded PCG64 Gaussian states, QR-orthonormalised)", "config": cfg,
         "gpu_launches": int(f["launches"]),
@@ -388,38 +574,56 @@ def main():
         e = res["e2e"]
         line["e2e"] = {"value": nwf_total * args.steps / (e["ms"] * 1e-3), "unit": metric,
                        "h2d_bytes_per_step": e["h2d"] / args.steps, "d2h_bytes_per_step": e["d2h"] / args.steps,
-                       "ms": e["ms"], "definition": "upload states (pinned) + initial measurement + K steps + "
-                       "download densities + energy, per K steps"}
+                       "ms": e["ms"], "ms_blocks": e["ms_blocks"],
+                       "definition": "upload states (pinned) + initial measurement + K steps + download densities + "
+                                     "energy, per K steps (median of the blocks)"}
     forms = {}
+    n = proj.numel
+    if "drift" in f:
+        forms["fp64"] = {"energy_drift": f["drift"]}
     for label in ("mixed_h64", "mixed_h32"):
-        if label in res:
+        if label in res and "unsupported" not in res[label]:
             m = res[label]
-            d64 = f["dens"]
-            n = proj.numel
-            rho = np.concatenate([d64[2 * n:3 * n], d64[7 * n:8 * n]])
-            rho_m = np.concatenate([m["dens"][2 * n:3 * n], m["dens"][7 * n:8 * n]])
-            forms[label] = {"value": nwf_total * args.steps / (m["ms"] * 1e-3),
+            forms[label] = {"value": nwf_total * args.steps / (m["ms"] * 1e-3), "ms_blocks": m["ms_blocks"],
                             "speedup_vs_fp64": f["ms"] / m["ms"],
-                            "density_rel_l2_err_vs_fp64": float(np.linalg.norm(rho_m - rho) / np.linalg.norm(rho)),
-                            "energy_rel_err_vs_fp64": float(abs(m["energy"][:7].sum() - f["energy"][:7].sum()) / abs(f["energy"][:7].sum())),
+                            "density_rel_l2_err_vs_fp64": rho_err(m["dens"], f["dens"], n),
+                            "energy_rel_err_vs_fp64": float(abs(total_energy(m["energy"]) - total_energy(f["energy"])) /
+                                                            abs(total_energy(f["energy"]))),
                             "ms_pass_a": m["ms_a"], "ms_pass_b": m["ms_b"]}
+            if "drift" in m:
+                forms[label]["energy_drift"] = m["drift"]
+                forms[label]["density_rel_l2_err_vs_fp64_after_drift_run"] = rho_err(m["drift_dens"], f["drift_dens"], n)
     if forms:
         line["precision_forms"] = forms
     if "adjoint" in res:
         line["adjoint"] = res["adjoint"]
     if not args.no_refcuda and world == 1:
         try:
-            line["reference_cuda"] = reference_cuda(proj.name, nwf, max(2, min(args.steps, 10)))
-            if line["reference_cuda"] and "value" in line["reference_cuda"]:
-                line["reference_cuda"]["note"] = "hpc-engine/*.cu compiled for sm_100a + oracle/ref_harness.cu, same GPU, same inputs"
+            rsteps = max(2, args.parity_steps if args.parity_steps > 0 else min(args.steps, 10))
+            ref = reference_cuda(proj.name, nwf, rsteps, (proj, d))
+            if ref and "value" in ref:
+                line["reference_cuda"] = {"value": ref["value"], "ms_per_step": ref["ms_per_step"], "steps": rsteps,
+                                          "note": "hpc-engine/*.cu compiled for sm_100a + oracle/ref_harness.cu, same GPU, "
+                                                  "same inputs"}
+                if args.parity_steps > 0:
+                    line["parity_full_size"] = parity_full_size(proj.name, nwf, rsteps, dev, (proj, d), ref)
+            else:
+                line["reference_cuda"] = ref
         except Exception as ex:  # reported, not fatal
             line["reference_cuda"] = {"error": str(ex)[:200]}
+    if args.extras and args.workload == "c2" and world == 1 and not args.nwf:
+        for key, fn in (("adjoint", adjoint_c4), ("c3", c3_comparison)):
+            try:
+                line[key] = fn(args, dev)
+            except Exception as ex:  # reported, not fatal
+                line[key] = {"error": f"{type(ex).__name__}: {str(ex)[:300]}"}
+            torch.cuda.empty_cache()
     if not args.no_cpu and world == 1:
         sample = CPU_SAMPLE[args.workload]
         line["cpu_baseline"] = cpu_baseline(proj.name, *sample)
+    line["wall_s"] = round(time.perf_counter() - t_start, 1)
     print(json.dumps(line))
     if world > 1:
-        import torch
         torch.distributed.destroy_process_group()
 
 

@@ -126,7 +126,9 @@ int density_caculate_tau(double *d_densities, int nthreads);
 int symmetrize_densities_device(double *d_densities);
 
 /* functional and H psi (hpc-engine/pca_kernels.cu:81, 674, 1020; cpca_kernels.cu:676;
- * ccpca_kernels.cu:625).  qfswitch > 0 (quantum friction) returns an error: not provided. */
+ * ccpca_kernels.cu:625).  qfswitch > 0 adds the quantum-friction terms built from the friction
+ * densities after the 12 N density words (pca_kernels.cu:497-539) to H, with pccoeff the
+ * particle-control coefficient. */
 int compute_potentials(int it, double *d_densities, double *d_potentials, double cccoeff, int nthreads);
 int multiply_wf_by_alpha(int n, wtd_z *wf_in, wtd_z *wf_out, double *d_potentials, int nthreads);
 #if WTD_CODEDIM == 3

@@ -6,7 +6,7 @@ regenerates the seeded inputs of wslda_b200.projects, runs the reference's time 
 saves the outputs as tests/golden/<project>.npz.  The fixtures pin the CPU oracle
 (tests/test_oracle_golden.py) and the CUDA library (tests/test_gpu_parity.py).
 
-    python tests/golden/make_golden.py --out gpurun_out/golden [project ...]
+    python tests/golden/make_golden.py --out <folder> [project ...]
 """
 import argparse
 import ctypes

@@ -32,7 +32,9 @@ sys.path.insert(0, os.path.dirname(HERE))
 from wslda_b200 import projects as P  # noqa: E402
 from td_gauss_util import GOLDEN, initial_states  # noqa: E402
 
-TESTSUITE = "/root/reference/testsuite"
+# the reference tree: WSLDA_REFERENCE, by default a "reference" folder beside the repository
+REFERENCE = os.environ.get("WSLDA_REFERENCE", os.path.join(REPO, os.pardir, "reference"))
+TESTSUITE = os.path.join(REFERENCE, "testsuite")
 
 
 def cases():

@@ -13,7 +13,7 @@ Hamiltonian"; 2026.09.25: "current-dependent mean fields").  These fixtures give
 reference's own trajectory for every case, so the library is pinned to it where the 2021 log
 no longer applies.
 
-    python tests/golden/make_td_gauss_refk.py --out gpurun_out/td_gauss_refk [--measurements M] [case ...]
+    python tests/golden/make_td_gauss_refk.py --out <folder> [--measurements M] [case ...]
 
 The 1D and 2D fixtures hold all 100 blocks; the 3D ones the first 20 (5,720 steps, 11,440 for
 SLDAE), which covers the ramp-up of the stirrer, to bound the reference's run time.

@@ -7,7 +7,8 @@ loss's rounding noise, ~1e-16 L / h, far below the gradient):
   - of the CUDA forward itself (the same library, loss-only calls),
   - of the CPU oracle's forward (an independent implementation of the step),
 to a relative tolerance of 1e-6, with several checkpoint intervals (segments of 1, 3 and all
-steps, a partial last segment included).
+steps, a partial last segment included).  The same gradient is also taken through the
+torch.autograd.Function of tests/adjoint_autograd.py, alone and inside a composite loss.
 """
 import numpy as np
 import pytest
@@ -174,3 +175,32 @@ def test_adjoint_unsupported_elsewhere(has_gpu):
     with pytest.raises(WtdError, match="not supported"):
         r.adjoint(2, nparam=1)
     r.close()
+
+
+@pytest.mark.gpu
+def test_adjoint_through_torch_autograd(setup_run):
+    """the torch.autograd.Function wrapper: backward() gives the adjoint gradient, which matches
+    finite differences of the wrapper's own forward, and the chain rule through a composite loss
+    (log(1 + L^2)) holds"""
+    import torch
+    from adjoint_autograd import StirrerLoss
+    proj, d, run, fresh = setup_run
+    m = _mask(proj)
+    th0 = np.array(d["params"][:NPARAM], dtype=np.float64)
+    theta = torch.tensor(th0, dtype=torch.float64, requires_grad=True)
+    loss = StirrerLoss.apply(theta, run, d, NSTEPS, m, 3)
+    loss.backward()
+    g = theta.grad.numpy().copy()
+
+    def loss_at(tp):
+        with torch.no_grad():
+            return float(StirrerLoss.apply(torch.tensor(tp), run, d, NSTEPS, m, 3))
+
+    fd = np.array([_richardson_fd(loss_at, th0, j) for j in range(NPARAM)])
+    assert rel(g, fd) < TOL, (g, fd)
+    # composite: d/dtheta log(1 + L^2) = 2 L / (1 + L^2) dL/dtheta
+    theta2 = torch.tensor(th0, dtype=torch.float64, requires_grad=True)
+    L = StirrerLoss.apply(theta2, run, d, NSTEPS, m, 0)
+    torch.log1p(L * L).backward()
+    lv = float(L.detach())
+    assert rel(theta2.grad.numpy(), 2 * lv / (1 + lv * lv) * g) < 1e-12

@@ -35,7 +35,22 @@ def _get(lib, p, n):
     return a
 
 
-def _densities(name, nwf, grads, weighted):
+def _plane_waves(proj, S, planewave):
+    """per-state plane-wave data of the 1D/2D engines: all zero, or (planewave) a mix of zero and
+    nonzero k_z (2D weight 1 or 2) and, in 1D, nonzero k_y, k_z with degeneracies cnt > 1"""
+    if not planewave:
+        return np.zeros(2 * S), np.ones(S, dtype=np.int32)
+    rng = np.random.Generator(np.random.PCG64(7))
+    k = rng.uniform(-0.8, 0.8, 2 * S)
+    k[::3] = 0.0                      # some states in the k_perp = 0 plane (weight 1)
+    if proj.codedim == 2:
+        k[S:] = 0.0                   # the 2D engine reads only k_z (first S entries)
+        k[1] = -np.pi / proj.dz       # the edge of the Brillouin zone (weight 1 with a cubic cut-off)
+    cnt = rng.integers(1, 7, S).astype(np.int32)
+    return k, cnt
+
+
+def _densities(name, nwf, grads, weighted, planewave=False):
     from wslda_b200 import load_library
     proj, d = inputs(name, nwf)
     lib = load_library(name)
@@ -45,8 +60,9 @@ def _densities(name, nwf, grads, weighted):
     dx, dy, dz, lap = (_dev(lib, np.zeros(M, dtype=np.complex128)) for _ in range(4))
     fb = _dev(lib, d["occ"])
     w = _dev(lib, np.linspace(0.5, 1.5, S)) if weighted else None
-    kk = _dev(lib, np.zeros(2 * S))
-    cnt = _dev(lib, np.ones(S, dtype=np.int32))
+    kk_h, cnt_h = _plane_waves(proj, S, planewave)
+    kk = _dev(lib, kk_h)
+    cnt = _dev(lib, cnt_h)
     outs = [_dev(lib, np.zeros(12 * N)) for _ in range(3)]
     assert lib.compute_derivatives(2 * S, wf, dx, dy, dz, lap, 512) == 0
     # the entry point that uses a caller-provided work area
@@ -73,11 +89,15 @@ def _densities(name, nwf, grads, weighted):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name,grads,weighted", [("t2d_slda", 1, False), ("t2d_slda", 0, True),
-                                                  ("t1d_custom", 1, True), ("t3d_slda", 1, False),
-                                                  ("c2_slda2d", 0, False)])
-def test_noalloc_densities_match_workspace_densities(has_gpu, name, grads, weighted):
-    N, (ref, first, second) = _densities(name, 24, grads, weighted)
+@pytest.mark.parametrize("name,grads,weighted,planewave", [
+    ("t2d_slda", 1, False, False), ("t2d_slda", 0, True, False), ("t1d_custom", 1, True, False),
+    ("t3d_slda", 1, False, False), ("c2_slda2d", 0, False, False),
+    # the plane-wave weights the kernel forms itself: 2D k_z != 0 counts twice, 1D states carry
+    # their degeneracy cnt and |k_perp|^2 enters tau
+    ("t2d_slda", 1, True, True), ("t2d_bdg", 1, False, True), ("t1d_custom", 1, False, True),
+    ("t1d_aslda", 1, True, True), ("t1d_sldae_a1", 1, False, True)])
+def test_noalloc_densities_match_workspace_densities(has_gpu, name, grads, weighted, planewave):
+    N, (ref, first, second) = _densities(name, 24, grads, weighted, planewave)
     assert np.linalg.norm(ref) > 0
     for got in (first, second):
         for k, v in density_errors(got, ref, N).items():

@@ -128,19 +128,13 @@ static int launch_pass_t(wtd_ctx *c, StepArgs &a)
     else {
         if (c->block == 1024 && WG::ntot >= 2048) {
             auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD, 1024>;
-            static bool attr = false;
-            if (!attr) {
-                WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                attr = true;
-            }
+            WTD_ONCE_PER_DEVICE(
+                WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)));
             k<<<c->grid, 1024, sm, c->st>>>(a, c->tw, c->ktab);
         } else {
             auto k = wtd_fused_pass<WG, TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD, 512>;
-            static bool attr = false;
-            if (!attr) {
-                WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                attr = true;
-            }
+            WTD_ONCE_PER_DEVICE(
+                WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)));
             int threads = WG::ntot >= 512 ? 512 : ((WG::ntot + 31) / 32) * 32;
             k<<<c->grid, threads, sm, c->st>>>(a, c->tw, c->ktab);
         }
@@ -218,8 +212,7 @@ static int filter_real(wtd_ctx *c, double *f, int nf)
     constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
     if (WTD_BIG) return big_filter_real(f, nf, c->hkf_mu, c->hkf_T, c->stage3d, c->tw, c->ktab, c->st);
     if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
-    static bool attr = false;
-    if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_hkf_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+    WTD_ONCE_PER_DEVICE(WTD_CU(cudaFuncSetAttribute(wtd_hkf_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)));
     wtd_hkf_kernel<WG><<<nf, 512, sm, c->st>>>(f, c->hkf_mu, c->hkf_T, c->tw, c->ktab);
     WTD_LAUNCHED(c);
     return WTD_OK;
@@ -246,8 +239,7 @@ static int filter_h(wtd_ctx *c, double *fld = NULL)
         if (WTD_BIG) return big_derivs(delta, 1, delta, NULL, NULL, NULL, c->tw, c->ktab, c->st, 1, c->hkf_mu, c->hkf_T);
         constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
         if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
-        static bool attr = false;
-        if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_hkf_c_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+        WTD_ONCE_PER_DEVICE(WTD_CU(cudaFuncSetAttribute(wtd_hkf_c_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)));
         wtd_hkf_c_kernel<WG><<<1, 512, sm, c->st>>>(delta, delta, c->hkf_mu, c->hkf_T, c->tw, c->ktab);
         WTD_LAUNCHED(c);
     }
@@ -279,8 +271,7 @@ static int coef_from_pots(wtd_ctx *c, int it, const double *fld = NULL)
     } else {
         constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
         if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
-        static bool attr = false;
-        if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_prep_var<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+        WTD_ONCE_PER_DEVICE(WTD_CU(cudaFuncSetAttribute(wtd_prep_var<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)));
         wtd_prep_var<WG><<<2, 256, sm, c->st>>>(c->cf, c->tw, c->ktab);
         WTD_LAUNCHED(c);
     }
@@ -348,8 +339,7 @@ static int after_pass(wtd_ctx *c, bool full, int it)
     if (full) {
         constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
         if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
-        static bool attr = false;
-        if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_tau_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+        WTD_ONCE_PER_DEVICE(WTD_CU(cudaFuncSetAttribute(wtd_tau_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)));
         wtd_tau_kernel<WG><<<2, 512, sm, c->st>>>(c->dens, c->tw, c->ktab);
         WTD_LAUNCHED(c);
     }
@@ -1138,8 +1128,7 @@ static int ss_derivs(wtd_ctx *c, SelfWork &w, const double2 *in, int grads)
     double2 *dx = grads ? w.ddx : NULL, *dy = (grads && CODEDIM >= 2) ? w.ddy : NULL, *dz = (grads && CODEDIM >= 3) ? w.ddz : NULL;
     if (WTD_BIG) return big_derivs_sep(in, nf, w.dlap, dx, dy, dz, NULL, NULL, c->tw, c->ktab, c->st);
     if (k_derivs_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
-    static bool attr = false;
-    if (!attr) { WTD_CU(cudaFuncSetAttribute(k_derivs<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k_derivs_smem)); attr = true; }
+    WTD_ONCE_PER_DEVICE(WTD_CU(cudaFuncSetAttribute(k_derivs<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k_derivs_smem)));
     k_derivs<WG><<<nf, 512, k_derivs_smem, c->st>>>(in, dx, dy, dz, w.dlap, c->tw, c->ktab);
     WTD_LAUNCHED(c);
     return WTD_OK;
@@ -1158,8 +1147,7 @@ static int ss_densities(wtd_ctx *c, SelfWork &w, const double2 *in, int grads)
     if (!grads) return WTD_OK;
     if (WTD_BIG) return big_tau(c->dens, c->stage3d, c->tw, c->ktab, c->st);
     constexpr size_t sm = (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>);
-    static bool attr = false;
-    if (!attr) { WTD_CU(cudaFuncSetAttribute(wtd_tau_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); attr = true; }
+    WTD_ONCE_PER_DEVICE(WTD_CU(cudaFuncSetAttribute(wtd_tau_kernel<WG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)));
     wtd_tau_kernel<WG><<<2, 512, sm, c->st>>>(c->dens, c->tw, c->ktab);
     WTD_LAUNCHED(c);
     return WTD_OK;
@@ -1583,12 +1571,9 @@ static int adjoint_run(wtd_ctx *c, int it0, int nsteps, int Kin, const double *m
     };
     auto kB = k_adj_B<WG, NH>;
     auto kA = k_adj_A<WG, NH>;
-    static bool attr = false;
-    if (!attr) {
+    WTD_ONCE_PER_DEVICE(
         WTD_CU(cudaFuncSetAttribute(kB, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        WTD_CU(cudaFuncSetAttribute(kA, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        attr = true;
-    }
+        WTD_CU(cudaFuncSetAttribute(kA, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)));
     /* the reverse kernels: one persistent CTA of 512 threads per SM (two CTAs of 256 per SM
      * measured the same); the slots hold c->grid * 12 N words, so up to 3 * c->grid CTAs of 4 N */
     const int threads = WG::ntot >= 512 ? 512 : ((WG::ntot + 31) / 32) * 32;

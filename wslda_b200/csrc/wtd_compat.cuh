@@ -11,6 +11,9 @@
  *   [0, S)            quasiparticle energies of the last apply_hamiltonian (pca.c:1575 reads them)
  *   [S', S'+18N)      per-point H coefficients (the CF_* list)
  *   [.., +G*12N)      density partial sums of the G CTAs of calculate_densities
+ *   [.., +2S')        per-state |k_perp|^2 and degeneracy weights of the plane-wave factor
+ *   [.., +2N)         scratch of compute_divergence_real_vector_f
+ * so the per-step calls of a driver that sized and set the work area allocate nothing.
  */
 #ifndef WTD_COMPAT_CUH
 #define WTD_COMPAT_CUH
@@ -25,6 +28,13 @@ static size_t compat_spad(void) { return ((size_t)(g_nwfip > 0 ? g_nwfip : 1) + 
 static double *compat_qpe(void) { return (double *)g_work; }
 static double *compat_cf(void) { return (double *)g_work + compat_spad(); }
 static double *compat_slots(void) { return (double *)g_work + compat_spad() + (size_t)CF_COUNT * WTD_NUMEL; }
+static double *compat_kpw(void) { return compat_slots() + (size_t)g_dens_grid * 12 * WTD_NUMEL; }
+static double *compat_divtmp(void) { return compat_kpw() + 2 * compat_spad(); }
+static size_t compat_work_words(void)
+{
+    return compat_spad() + (size_t)CF_COUNT * WTD_NUMEL + (size_t)g_dens_grid * 12 * WTD_NUMEL + 2 * compat_spad() +
+           2 * (size_t)WTD_NUMEL;
+}
 
 static int cu_sync_status(void)
 {
@@ -508,16 +518,29 @@ __global__ void k_planewave(int n, const double *kky, const double *kkz, const i
 #endif
 }
 
+/* the per-state plane-wave arrays of the current call: in the work area when it is set and
+ * sized for n states; otherwise (calculate_quantum_friction_densities before the work area is
+ * set) in a library-owned pair that is allocated when it first has to grow */
 static double *g_kp2 = NULL, *g_wcnt = NULL;
-static int g_kp_n = 0;
+static double *g_kp2_own = NULL, *g_wcnt_own = NULL;
+static int g_kp_own_n = 0;
 static int compat_planewave(int n, const double *kky, const double *kkz, const int *cnt)
 {
-    if (g_kp_n < n) {
-        if (g_kp2) cudaFree(g_kp2);
-        if (g_wcnt) cudaFree(g_wcnt);
-        if (cudaMalloc((void **)&g_kp2, n * sizeof(double)) != cudaSuccess) return WTD_ERR_NOMEM;
-        if (cudaMalloc((void **)&g_wcnt, n * sizeof(double)) != cudaSuccess) return WTD_ERR_NOMEM;
-        g_kp_n = n;
+    if (g_work && n <= g_nwfip) {
+        g_kp2 = compat_kpw();
+        g_wcnt = g_kp2 + compat_spad();
+    } else {
+        if (g_kp_own_n < n) {
+            if (g_kp2_own) cudaFree(g_kp2_own);
+            if (g_wcnt_own) cudaFree(g_wcnt_own);
+            g_kp2_own = g_wcnt_own = NULL;
+            g_kp_own_n = 0;
+            if (cudaMalloc((void **)&g_kp2_own, n * sizeof(double)) != cudaSuccess) return WTD_ERR_NOMEM;
+            if (cudaMalloc((void **)&g_wcnt_own, n * sizeof(double)) != cudaSuccess) return WTD_ERR_NOMEM;
+            g_kp_own_n = n;
+        }
+        g_kp2 = g_kp2_own;
+        g_wcnt = g_wcnt_own;
     }
     k_planewave<<<(n + 127) / 128, 128>>>(n, kky, kkz, cnt, g_kp2, g_wcnt);
     return 0;
@@ -553,12 +576,14 @@ static int noalloc_scratch(double **out)
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return WTD_ERR_CUDA;
     if (dev < 0 || dev >= 64) return WTD_ERR_ARG;
-    if (!g_noalloc_scratch[dev]) {
-        double *p = NULL;
+    /* host threads may race on the first call; each stores the same address (atomic access
+     * keeps every read whole) */
+    double *p = __atomic_load_n(&g_noalloc_scratch[dev], __ATOMIC_ACQUIRE);
+    if (!p) {
         if (cudaGetSymbolAddress((void **)&p, wtd_noalloc_scratch) != cudaSuccess || !p) return WTD_ERR_CUDA;
-        g_noalloc_scratch[dev] = p;
+        __atomic_store_n(&g_noalloc_scratch[dev], p, __ATOMIC_RELEASE);
     }
-    *out = g_noalloc_scratch[dev];
+    *out = p;
     return WTD_OK;
 }
 
@@ -687,7 +712,7 @@ int create_cufftPlans(int batch_size, int nwfip, size_t *workSize)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     g_dens_grid = nsm * 2 < nwfip ? nsm * 2 : nwfip;
-    size_t need = compat_spad() + (size_t)CF_COUNT * WTD_NUMEL + (size_t)g_dens_grid * 12 * WTD_NUMEL;
+    size_t need = compat_work_words();
     size_t ref = (size_t)(24 + 8) * WTD_NUMEL;  /* PCA_WORKSPACE_SHIFT + PCA_DERIVATIVE_SHIFT */
     *workSize = sizeof(double) * (need > ref ? need : ref);
     return compat_tables();
@@ -774,10 +799,21 @@ int compute_derivative_real_vector_f(double *fx, double *fy, double *fz, double 
     if (!r && CODEDIM >= 3 && fz) r = compat_real_deriv(fz, dfz_dz, 3);
     return r;
 }
+/* scratch of the divergence: the work area's 2 N words, or (work area not yet set) a
+ * library-owned array allocated on the first such call and kept */
+static double *g_divtmp_own = NULL;
 int compute_divergence_real_vector_f(double *fx, double *fy, double *fz, double *divf, int nthreads)
 {
     double *t = NULL;
-    if (cudaMalloc((void **)&t, 2 * sizeof(double) * WTD_NUMEL) != cudaSuccess) return WTD_ERR_NOMEM;
+    if (g_work) {
+        t = compat_divtmp();
+    } else {
+        if (!g_divtmp_own && cudaMalloc((void **)&g_divtmp_own, 2 * sizeof(double) * WTD_NUMEL) != cudaSuccess) {
+            g_divtmp_own = NULL;
+            return WTD_ERR_NOMEM;
+        }
+        t = g_divtmp_own;
+    }
     int r = compat_real_deriv(fx, divf, 1);
     if (!r && CODEDIM >= 2) { r = compat_real_deriv(fy, t, 2); }
     if (!r && CODEDIM >= 3) { r = compat_real_deriv(fz, t + WTD_NUMEL, 3); }
@@ -785,7 +821,6 @@ int compute_divergence_real_vector_f(double *fx, double *fy, double *fz, double 
         k_add_fields<<<(WTD_NUMEL + 255) / 256, 256>>>(divf, t, CODEDIM >= 3 ? t + WTD_NUMEL : NULL, WTD_NUMEL);
         r = cu_sync_status();
     }
-    cudaFree(t);
     return r;
 }
 

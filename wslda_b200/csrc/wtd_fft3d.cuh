@@ -118,14 +118,10 @@ static int big_derivs(double2 *in, int nf, double2 *lap, double2 *dx, double2 *d
 {
     constexpr int NYZ = NY * NZ, N = NX * NY * NZ;
     if (NYZ % WTD_PX != 0) return WTD_ERR_UNSUPPORTED;
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(k_planes<WGP, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)planes_smem) != cudaSuccess ||
-            cudaFuncSetAttribute(k_planes<WGP, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)planes_smem) != cudaSuccess ||
-            cudaFuncSetAttribute(k_pencils<WGX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pencils_smem) != cudaSuccess)
-            return WTD_ERR_CUDA;
-        attr = true;
-    }
+    WTD_ONCE_PER_DEVICE(
+        WTD_CU(cudaFuncSetAttribute(k_planes<WGP, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)planes_smem));
+        WTD_CU(cudaFuncSetAttribute(k_planes<WGP, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)planes_smem));
+        WTD_CU(cudaFuncSetAttribute(k_pencils<WGX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pencils_smem)));
     /* forward (y, z) into the laplacian buffer (in place when there is none: the input is then
      * overwritten by its transform) */
     double2 *K = lap ? lap : in;
@@ -292,15 +288,11 @@ static int big_derivs_sep(const double2 *in, int nf, double2 *lap, double2 *dx, 
     if (NYZ % WTD_PXS != 0) return WTD_ERR_UNSUPPORTED;
     if (sep_planes_smem > WTD_SMEM_MAX || sep_pencils_smem > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     if (in == lap || in == dx || in == dy || in == dz) return WTD_ERR_ARG;
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(k_sep_planes<WGP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sep_planes_smem) != cudaSuccess ||
-            cudaFuncSetAttribute(k_sep_planes<WGP>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
-            cudaFuncSetAttribute(k_sep_pencils<WGXS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sep_pencils_smem) != cudaSuccess)
-            return WTD_ERR_CUDA;
-        attr = true;
-    }
+    WTD_ONCE_PER_DEVICE(
+        WTD_CU(cudaFuncSetAttribute(k_sep_planes<WGP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sep_planes_smem));
+        WTD_CU(cudaFuncSetAttribute(k_sep_planes<WGP>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared));
+        WTD_CU(cudaFuncSetAttribute(k_sep_pencils<WGXS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sep_pencils_smem)));
     const int nfa = nf / 2;
     if (lap || dy || dz)
         k_sep_planes<WGP><<<nf * NX, WTD_SEP_NT, sep_planes_smem, st>>>(in, lap, dy, dz, wa, wb, nfa, tw + NX, ktab);

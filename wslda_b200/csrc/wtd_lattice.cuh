@@ -36,6 +36,22 @@ static inline int wtd_cuerr(cudaError_t e) { return e == cudaSuccess ? WTD_OK : 
 #define WTD_TRY(x) do { int _r = (x); if (_r) return _r; } while (0)
 #define WTD_CU(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return WTD_ERR_CUDA; } while (0)
 
+/* statements run once per device (kernel attributes such as the dynamic shared-memory size are
+ * per-device settings, and contexts may live on different devices of one process); devices
+ * beyond WTD_MAXDEV run them on every call */
+#define WTD_MAXDEV 64
+#define WTD_ONCE_PER_DEVICE(...)                                                  \
+    do {                                                                          \
+        static bool _wtd_once[WTD_MAXDEV];                                        \
+        int _wtd_dev = -1;                                                        \
+        if (cudaGetDevice(&_wtd_dev) != cudaSuccess) return WTD_ERR_CUDA;         \
+        const bool _wtd_slot = _wtd_dev >= 0 && _wtd_dev < WTD_MAXDEV;            \
+        if (!_wtd_slot || !_wtd_once[_wtd_dev]) {                                 \
+            __VA_ARGS__;                                                          \
+            if (_wtd_slot) _wtd_once[_wtd_dev] = true;                            \
+        }                                                                         \
+    } while (0)
+
 /* FFT twiddles e^{-2 pi i t/n} per axis and wave-number tables of digit-reversed positions
  * (rows 0-2 k_d, rows 3-5 k_d with the Nyquist mode zeroed) for this lattice */
 static void wtd_make_tables(double2 *tw, double *kt)
