@@ -38,8 +38,10 @@ WORKLOADS = {
     "c1": dict(project="c1_bdg1d", nwf=256, desc="1D TD-BdG NX=128, 256 states, AB3AM4"),
     "c4": dict(project="c4_bdg2d", nwf=4608, desc="2D TD-BdG 48x48, 4608 states, AB3AM4, stirrer"),
     "c3": dict(project="c3_aslda3d", nwf=12000, desc="3D TD-ASLDA 32^3, 12000 states, AB5AM5, 5% spin imbalance, "
-               "Delta_ext 0.2 with 1% noise (plane/pencil path)", forms=("fp64", "mixed_h64")),
+               "Delta_ext 0.2 with 1% noise (3D line path)"),
 }
+C5 = dict(project="c5_slda3d", nwf=20000, desc="3D TD-SLDA 48^3 vortex with a moving Gaussian stirrer, AB3AM4, "
+          "complex64 states and history (3D line path)")
 
 
 # DRAM bytes (read + write) per state of the FP64 passes, from one ncu capture of the same
@@ -440,20 +442,110 @@ def c3_comparison(args, dev):
     return out
 
 
-def cpu_baseline(name, nwf_sample, steps, threads=None):
-    """CPU oracle port on the host cores: bounded sample of the workload."""
+def cpu_baseline(name, nwf_sample, steps, threads=None, single_thread=True):
+    """The step on the host cores, bounded sample of the workload.  Where it is built (it ships
+    in oracle/_ref/<project>/liboracle_wderiv.so), the spectral derivatives are the reference's
+    own CPU library, lib/wderiv/c/wderiv.c compiled unmodified over an in-repo FFTW3-API shim
+    (FFTW is not installed), with the oracle's restatement of the local update, densities,
+    functional and ABM; else the oracle port alone.  OpenMP over states on all host threads,
+    and a one-thread figure of the same sample."""
+    import platform
     from parity_util import inputs
     from oracle_lib import Oracle
     threads = threads or os.cpu_count()
+    so = os.path.join(REPO, "oracle", "_ref", name, "liboracle_wderiv.so")
+    variant = "wderiv" if os.path.exists(so) else None
     proj, d = inputs(name, nwf_sample)
-    o = Oracle(name, threads=threads)
-    o.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
-    o.initial_measurement()
-    t0 = time.perf_counter()
-    o.steps(steps)
-    dt = time.perf_counter() - t0
-    return {"value": nwf_sample * steps / dt, "unit": "qp-state*steps/s", "cores": threads, "kind": "port",
-            "sample": f"{nwf_sample} of the workload's states x {steps} steps, {dt:.1f} s, oracle/wtd_oracle.cpp"}
+
+    def run(th, nsteps):
+        o = Oracle(name, threads=th, variant=variant)
+        o.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+        o.initial_measurement()
+        t0 = time.perf_counter()
+        o.steps(nsteps)
+        return time.perf_counter() - t0
+
+    dt = run(threads, steps)
+    cpu = platform.processor() or ""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            cpu = next((l.split(":", 1)[1].strip() for l in fh if l.startswith("model name")), cpu)
+    except Exception:
+        pass
+    out = {"value": nwf_sample * steps / dt, "unit": "qp-state*steps/s", "cores": threads,
+           "kind": "reference" if variant else "port", "cpu": cpu,
+           "sample": f"{nwf_sample} of the workload's states x {steps} steps, {dt:.1f} s, " +
+                     ("wderiv (lib/wderiv/c/wderiv.c) + in-repo FFT shim (FFTW unavailable) + the oracle's local update"
+                      if variant else "oracle/wtd_oracle.cpp")}
+    if single_thread:
+        s1 = max(1, steps // 8)
+        dt1 = run(1, s1)
+        out["value_1_thread"] = nwf_sample * s1 / dt1
+        out["sample_1_thread"] = f"{nwf_sample} states x {s1} steps, {dt1:.1f} s"
+    return out
+
+
+def c5_scale(args, dev):
+    """The 3D TD-SLDA vortex workload (48^3, AB3AM4) in the all-FP32 storage form (complex64
+    states and history, FP32 transforms, FP64 sums) at the largest state count that fits the
+    GPU, up to the workload's 20,000; and its error against FP64 on a subset of states."""
+    import torch
+    from wslda_b200 import TDRun, projects as P
+    name = C5["project"]
+    proj = P.Project(name)
+    free, _ = torch.cuda.mem_get_info(dev)
+    per_state = 2 * proj.numel * 8 * (1 + proj.nhist + 1)     # y, the ring, K_yz (complex64)
+    nwf = int(min(C5["nwf"], args.c5_nwf or C5["nwf"], (free - (6 << 30)) // per_state))
+    out = {"workload": C5["desc"], "states_requested": C5["nwf"], "states": nwf,
+           "resident_bytes_per_state": per_state, "steps": args.c5_steps, "blocks": args.blocks}
+    # the full state count as host FP64 would be 2 x 20,000 x 110,592 complex128 (70 GB) and its
+    # QR beyond one GPU: the states are seeded Gaussian complex64 drawn on the device in chunks
+    # (torch Philox, seed 20261203 + 5) straight into the context's state array; the initial
+    # measurement normalises each state
+    import ctypes
+    seed = P.config_seed(name)
+    r = TDRun(name, nwf, precision=2, device=dev)
+    sp = ctypes.c_void_p()
+    r._check(r.lib.wtd_device_pointers(r.h, ctypes.byref(sp), None, None))
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    n2 = 2 * nwf * proj.numel
+    chunk = 1 << 27
+    for o in range(0, n2, chunk):
+        m = min(chunk, n2 - o)
+        z = torch.randn(2 * m, device="cuda", dtype=torch.float32, generator=g)
+        r.lib.memcopy_gpu2gpu(ctypes.c_void_p(z.data_ptr()), ctypes.c_void_p(sp.value + 8 * o), ctypes.c_size_t(8 * m))
+        del z
+    torch.cuda.synchronize()
+    r.setup_fields(P.make_potentials(proj), P.make_occupations(nwf), proj.params, P.make_extra(proj, seed))
+    r.initial_measurement()
+    r.steps(args.warmup)
+    r.sync()
+    stream = torch.cuda.ExternalStream(r.stream())
+    t = timed_blocks(r, stream, args.c5_steps, args.blocks, dev, 1)
+    r.close()
+    ba, bb = pass_bytes(proj, 2)
+    hbm, _ = peaks()
+    out.update({"value": nwf * args.c5_steps / (t["ms"] * 1e-3), "ms_per_step": t["ms"] / args.c5_steps,
+                "ms_blocks": t["ms_blocks"], "hbm_gbs_compulsory": (ba + bb) * nwf * args.c5_steps / (t["ms"] * 1e-3) / 1e9,
+                "clocks": t["clocks"]})
+    out["roofline_frac"] = out["hbm_gbs_compulsory"] / hbm
+    # accuracy against FP64 on a subset of the workload
+    ns = args.c5_err_nwf
+    pe, de = make_inputs(name, ns)
+    res = {}
+    for label, prec in (("fp64", 0), ("mixed_h32", 2)):
+        rr = TDRun(name, ns, precision=prec, device=dev)
+        rr.setup(de["states"], de["pots"], de["occ"], de["params"], de["extra"])
+        rr.initial_measurement()
+        rr.steps(args.c5_err_steps)
+        res[label] = (rr.densities(), rr.energy())
+        rr.close()
+    out["error_vs_fp64"] = {"states": ns, "steps": args.c5_err_steps,
+                            "density_rel_l2": rho_err(res["mixed_h32"][0], res["fp64"][0], pe.numel),
+                            "energy_rel": abs(total_energy(res["mixed_h32"][1]) - total_energy(res["fp64"][1])) /
+                                          abs(total_energy(res["fp64"][1]))}
+    return out
 
 
 def adjoint_c4(args, dev):
@@ -497,6 +589,10 @@ def main():
     ap.add_argument("--c3-drift-nwf", type=int, default=1024)
     ap.add_argument("--c3-parity-nwf", type=int, default=4000)
     ap.add_argument("--c3-parity-steps", type=int, default=10)
+    ap.add_argument("--c5-nwf", type=int, default=0)
+    ap.add_argument("--c5-steps", type=int, default=3)
+    ap.add_argument("--c5-err-nwf", type=int, default=256)
+    ap.add_argument("--c5-err-steps", type=int, default=20)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     args.blocks = max(args.blocks, 1)
@@ -515,7 +611,7 @@ def main():
         cb = None
         t0 = time.perf_counter()
         for k in range(max(1, min(args.steps, 3))):
-            cb = cpu_baseline(wl["project"], sample[0], sample[1])
+            cb = cpu_baseline(wl["project"], sample[0], sample[1], single_thread=False)
             vals.append(cb["value"])
         v = float(np.median(vals))
         cb["value"] = v
@@ -525,7 +621,8 @@ def main():
                 "data": "synthetic", "config": cfg, "cpu_baseline": cb,
                 "e2e": {"value": v, "unit": metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "note": "the reference has no CPU implementation of the TD step (td codes require GPUs); this arm "
-                        "times the CPU restatement of the reference step (oracle port) on all host threads",
+                        "times the step on all host threads with the reference's own CPU derivative library "
+                        "(lib/wderiv) and the oracle's restatement of the rest of the step",
                 "wall_s": round(time.perf_counter() - t0, 1)}
         print(json.dumps(line))
         return
@@ -612,7 +709,7 @@ def main():
         except Exception as ex:  # reported, not fatal
             line["reference_cuda"] = {"error": str(ex)[:200]}
     if args.extras and args.workload == "c2" and world == 1 and not args.nwf:
-        for key, fn in (("adjoint", adjoint_c4), ("c3", c3_comparison)):
+        for key, fn in (("adjoint", adjoint_c4), ("c3", c3_comparison), ("c5", c5_scale)):
             try:
                 line[key] = fn(args, dev)
             except Exception as ex:  # reported, not fatal

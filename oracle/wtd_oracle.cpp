@@ -165,6 +165,62 @@ static inline double kval(int ax, int i)
     return (i < n / 2) ? 2. * M_PI / AXL[ax] * (double)i : 2. * M_PI / AXL[ax] * (double)(i - n);
 }
 
+#ifdef ORACLE_WDERIV
+/* Host-core baseline build (make -C oracle wderiv): the spectral derivatives of the states come
+ * from the reference's own CPU library, lib/wderiv/c/wderiv.c, compiled unmodified over the
+ * FFTW3-API shim of oracle/fftw_shim (FFTW is not installed).  wderiv_*_c take C99 double
+ * complex arrays, which have std::complex<double>'s layout. */
+extern "C" {
+int wderiv_init_3d(int nx, int ny, int nz, double dx, double dy, double dz);
+int wderiv_init_2d(int nx, int ny, double dx, double dy);
+int wderiv_init_1d(int nx, double dx);
+int wderiv_gradient_3d_c(void *f, void *dfdx, void *dfdy, void *dfdz);
+int wderiv_gradient_2d_c(void *f, void *dfdx, void *dfdy);
+int wderiv_gradient_1d_c(void *f, void *dfdx);
+int wderiv_laplace_3d_c(void *f, void *laplace);
+int wderiv_laplace_2d_c(void *f, void *laplace);
+int wderiv_laplace_1d_c(void *f, void *laplace);
+int wderiv_dfdx_3d_c(void *f, void *d);
+int wderiv_dfdy_3d_c(void *f, void *d);
+int wderiv_dfdz_3d_c(void *f, void *d);
+int wderiv_dfdx_2d_c(void *f, void *d);
+int wderiv_dfdy_2d_c(void *f, void *d);
+int wderiv_dfdx_1d_c(void *f, void *d);
+}
+static int wderiv_ready = [] {
+#if CODEDIM == 3
+    return wderiv_init_3d(NX, NY, NZ, DX, DY, DZ);
+#elif CODEDIM == 2
+    return wderiv_init_2d(NX, NY, DX, DY);
+#else
+    return wderiv_init_1d(NX, DX);
+#endif
+}();
+
+/* compute_derivatives for one complex field through wderiv: d/dx_d (odd derivative, Nyquist
+ * mode zeroed) and the laplacian as the sum of the second derivatives, each 1/N normalised
+ * (wderiv.c:503-567, the same multipliers as pca_derivative.cu:139-277) */
+static void derivs_one(const Complex *f, Complex *dx, Complex *dy, Complex *dz, Complex *lap)
+{
+    (void)wderiv_ready;
+    void *in = (void *)f;
+#if CODEDIM == 3
+    if (dx) wderiv_dfdx_3d_c(in, dx);
+    if (dy) wderiv_dfdy_3d_c(in, dy);
+    if (dz) wderiv_dfdz_3d_c(in, dz);
+    if (lap) wderiv_laplace_3d_c(in, lap);
+#elif CODEDIM == 2
+    (void)dz;
+    if (dx) wderiv_dfdx_2d_c(in, dx);
+    if (dy) wderiv_dfdy_2d_c(in, dy);
+    if (lap) wderiv_laplace_2d_c(in, lap);
+#else
+    (void)dy; (void)dz;
+    if (dx) wderiv_dfdx_1d_c(in, dx);
+    if (lap) wderiv_laplace_1d_c(in, lap);
+#endif
+}
+#else
 /* compute_derivatives for one complex field (pca_derivative.cu:139-277): d/dx_d with the
  * Nyquist mode zeroed, laplacian without; 1/N folded into the k factors. Any output may be
  * null. */
@@ -197,6 +253,7 @@ static void derivs_one(const Complex *f, Complex *dx, Complex *dy, Complex *dz, 
         std::copy(G.begin(), G.end(), lap);
     }
 }
+#endif
 
 /* laplacian / d f_d/dx_d of real fields (pca_derivative.cu:490-700, D2Z/Z2D); the complex
  * transform of a real field gives the same real result. */

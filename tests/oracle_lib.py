@@ -30,15 +30,33 @@ def _stale(so):
     return any(os.path.exists(f) and os.path.getmtime(f) > t for f in srcs)
 
 
+def wderiv_library(project):
+    """the wderiv baseline library of a project, built when the reference tree is present;
+    None when it is neither built nor buildable"""
+    so = os.path.join(ORACLE_DIR, "_ref", project, "liboracle_wderiv.so")
+    ref = os.environ.get("WSLDA_REFERENCE", os.path.join(REPO, os.pardir, "reference"))
+    if os.path.isdir(os.path.join(ref, "lib", "wderiv")):
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR, "wderiv", f"PROJECT={project}"], check=True)
+    return so if os.path.exists(so) else None
+
+
 class Oracle:
     """One oracle instance per project (a separate process-level library, as it keeps state)."""
 
-    def __init__(self, project, threads=None):
+    def __init__(self, project, threads=None, variant=None):
+        """variant "wderiv": the host-core baseline build, whose state derivatives come from the
+        reference's lib/wderiv (oracle/_ref/<project>/liboracle_wderiv.so, made by
+        `make -C oracle wderiv PROJECT=<project>` where the reference tree is present)"""
         from wslda_b200.projects import Project
         self.proj = Project(project)
-        so = os.path.join(ORACLE_DIR, "_build", project, "liboracle.so")
-        if _stale(so):
-            build(project)
+        if variant == "wderiv":
+            so = wderiv_library(project)
+            if so is None:
+                raise FileNotFoundError(f"no wderiv build of {project}")
+        else:
+            so = os.path.join(ORACLE_DIR, "_build", project, "liboracle.so")
+            if _stale(so):
+                build(project)
         self.lib = ctypes.CDLL(so, mode=ctypes.RTLD_LOCAL)
         L = self.lib
         for fn in ("orc_numel", "orc_codedim", "orc_nhist", "orc_functional", "orc_const_mass", "orc_get_it",

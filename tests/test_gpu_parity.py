@@ -56,12 +56,13 @@ def test_variable_mass_many_states(has_gpu, name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,nwf,prec,tol", [("t2d_slda", 24, 1, 1e-5), ("t2d_slda", 24, 2, 1e-5), ("t3d_aslda", 24, 1, 1e-5),
-                                                ("c3_aslda3d", 8, 1, 1e-6), ("t2d_big", 8, 1, 1e-6)])
+                                                ("c3_aslda3d", 8, 1, 1e-5), ("c3_aslda3d", 8, 2, 1e-5),
+                                                ("c5_slda3d", 4, 1, 1e-5), ("c5_slda3d", 4, 2, 1e-5), ("t2d_big", 8, 1, 1e-6)])
 def test_mixed_forms_track_fp64(has_gpu, name, nwf, prec, tol):
     """the FP32-mixed forms (complex64 states; FP64 or complex64 history) against the FP64
-    oracle over a measurement block: the fused lattices compute FFT and H psi in FP32, the
-    plane/pencil lattices (c3_aslda3d, t2d_big) keep FP64 arithmetic and round the states to
-    complex64 after each renormalisation"""
+    oracle over a measurement block: the fused lattices and the 3D line path (c3_aslda3d,
+    c5_slda3d) compute the transforms and H psi in FP32; the 2D plane/pencil lattice (t2d_big)
+    keeps FP64 arithmetic and rounds the states to complex64 after each renormalisation"""
     o = run_oracle(name, nwf, 3, 1)
     g = run_gpu(name, nwf, 3, 1, precision=prec)
     n = o["densities"].size // 12
@@ -74,9 +75,10 @@ def test_mixed_forms_track_fp64(has_gpu, name, nwf, prec, tol):
 
 @pytest.mark.gpu
 def test_mixed_h32_refused_on_plane_pencil_path(has_gpu):
+    """complex64 history needs FP32 arithmetic, which the 2D plane/pencil path does not have"""
     from wslda_b200 import TDRun, WtdError
     with pytest.raises(WtdError):
-        TDRun("c3_aslda3d", 8, precision=2)
+        TDRun("t2d_big", 8, precision=2)
 
 
 @pytest.mark.gpu
@@ -90,14 +92,19 @@ def test_c4_bdg2d_small_s(has_gpu):
 
 
 @pytest.mark.gpu
-def test_c3_aslda3d_small_s(has_gpu):
-    """3D ASLDA 32^3 (state larger than one CTA): the staged plane/pencil path."""
+@pytest.mark.parametrize("path", ["staged", "line"])
+def test_c3_aslda3d_small_s(has_gpu, monkeypatch, path):
+    """3D ASLDA 32^3 (state larger than one CTA) in FP64: the staged plane/pencil path (the FP64
+    default) and the 3D line path (the FP32 forms' path)"""
+    monkeypatch.setenv("WTD_3D_PATH", path)
     _compare("c3_aslda3d", nwf=8, nsteps=2, nmeas=1)
 
 
 @pytest.mark.gpu
-def test_c5_slda3d_small_s(has_gpu):
-    """3D SLDA 48^3 (radix-3 axes) through the staged path."""
+@pytest.mark.parametrize("path", ["staged", "line"])
+def test_c5_slda3d_small_s(has_gpu, monkeypatch, path):
+    """3D SLDA 48^3 (radix-3 axes) in FP64 on both 3D paths."""
+    monkeypatch.setenv("WTD_3D_PATH", path)
     _compare("c5_slda3d", nwf=4, nsteps=2, nmeas=1)
 
 

@@ -91,3 +91,27 @@ def test_oracle_high_k_filter_matches_numpy(project):
     c = o.filter_field(np.full(proj.numel, 2.0))
     assert np.allclose(c, 2.0 / (np.exp(-mu / T) + 1.0), rtol=1e-13)
     o.set_high_k_filter(0, 0.0, 1.0)
+
+
+@pytest.mark.parametrize("name", ["c2_slda2d", "t1d_aslda", "t3d_aslda", "c4_bdg2d"])
+def test_wderiv_baseline_matches_oracle(name):
+    """the host-core baseline (the reference's lib/wderiv derivatives over the in-repo FFTW-API
+    shim, with the oracle's local update) reproduces the oracle's step: densities, energies and
+    states after a few steps at 1e-12"""
+    from oracle_lib import Oracle, wderiv_library
+    from parity_util import density_errors, inputs, rel
+    if wderiv_library(name) is None:
+        pytest.skip("wderiv baseline not built (reference tree absent)")
+    proj, d = inputs(name, 12)
+    out = []
+    for variant in (None, "wderiv"):
+        o = Oracle(name, threads=2, variant=variant)
+        o.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+        o.initial_measurement()
+        o.steps(3)
+        out.append((o.densities(), o.energy(), o.states()))
+    (d0, e0, s0), (d1, e1, s1) = out
+    for k, v in density_errors(d1, d0, proj.numel).items():
+        assert v < 1e-12, (k, v)
+    assert rel(e1[:9], e0[:9]) < 1e-12
+    assert rel(s1, s0) < 1e-12

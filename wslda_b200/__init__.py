@@ -150,6 +150,11 @@ class TDRun:
             pass
 
     def setup(self, states, pots, occ, params, extra=None, const=None, it0=0, kky=None, kkz=None, cnt=None):
+        self.upload_states(states)
+        self.setup_fields(pots, occ, params, extra, const, it0, kky, kkz, cnt)
+
+    def setup_fields(self, pots, occ, params, extra=None, const=None, it0=0, kky=None, kkz=None, cnt=None):
+        """everything of setup() but the states (for states written on the device directly)"""
         c = const or self.proj.constants()
         self._check(self.lib.wtd_set_constants(self.h, c["mu_a"], c["mu_b"], c["ec"], c["t0"], c["dt"], c["kF"]))
         self._check(self.lib.wtd_set_sclgth(self.h, c["sclgth"]))
@@ -157,7 +162,6 @@ class TDRun:
         self._check(self.lib.wtd_set_params(self.h, _p(self._params)))
         ex = np.ascontiguousarray(extra if extra is not None else np.zeros(0), dtype=np.float64)
         self._check(self.lib.wtd_set_extra_data(self.h, ex.ctypes.data if ex.size else None, ex.nbytes))
-        self.upload_states(states)
         self._check(self.lib.wtd_upload_potentials(self.h, _p(np.ascontiguousarray(pots, dtype=np.float64))))
         cnt_p = None if cnt is None else np.ascontiguousarray(cnt, dtype=np.int32).ctypes.data_as(_ip)
         kky = None if kky is None else np.ascontiguousarray(kky, dtype=np.float64)

@@ -41,9 +41,17 @@ struct wtd_ctx {
     int timing;
     cudaEvent_t ev[2][2][4096];
     int nev[2];
-    /* large 3D lattices (state larger than one CTA's shared memory): staged path */
+    /* large 3D lattices (state larger than one CTA's shared memory): the line path
+     * (wtd_path3d.cuh), or the staged path where the line path does not apply (quantum
+     * friction, large 2D lattices) */
     int staged;
     double2 *ddx, *ddy, *ddz, *dlap, *dalap, *stage3d;
+    int line;                   /* line path in use */
+    void *kbuf;                 /* K_yz of every state, compute precision */
+    int ncl;                    /* clusters of the x-line kernel */
+    int g2;                     /* state chunks of the plane density kernel */
+    int p1grid;                 /* CTAs of the plane H kernel */
+    void *xfer;                 /* bounded staging buffer of the mixed-precision uploads/downloads */
     /* state-sharded runs: sum of the density partials over ranks (NCCL or a host hook) */
     void *nccl;
     wtd_exchange_fn xfn;
@@ -110,6 +118,9 @@ static int exchange(wtd_ctx *c, double *buf, size_t count)
     }
     return WTD_OK;
 }
+
+/* complex numbers per chunk of the mixed-precision uploads and downloads (64 MiB of FP64) */
+#define WTD_XFER ((size_t)1 << 22)
 
 static size_t elem_bytes_y(int prec) { return prec == WTD_FP64 ? sizeof(double2) : sizeof(float2); }
 static size_t elem_bytes_h(int prec) { return prec == WTD_MIXED_H32 ? sizeof(float2) : sizeof(double2); }
@@ -189,13 +200,16 @@ static int run_pass(wtd_ctx *c, int pass, bool grad)
     return grad ? launch_pass<2, true>(c, a) : launch_pass<2, false>(c, a);
 }
 
+static int line_pass(wtd_ctx *c, int pass, bool grad, const StepArgs *given = NULL);
+
 /* f1 = (H - <H>) psi of the current state and its quasiparticle energies, as the reference
  * leaves them after a step (pca.c:1565, d_workarea[0..n)); later steps reuse f1 */
 static int ensure_fk(wtd_ctx *c)
 {
     if (c->fk_given) return WTD_OK;
     if (!c->have_coef) return WTD_ERR_STATE;
-    WTD_TRY(run_pass(c, 3, false));
+    if (c->line) WTD_TRY(line_pass(c, 3, false));
+    else WTD_TRY(run_pass(c, 3, false));
     c->fk_given = 1;
     return WTD_OK;
 }
@@ -514,6 +528,238 @@ static int staged_step(wtd_ctx *c, bool last)
     return WTD_OK;
 }
 
+/* ---------------------------------------------------------------------------------------
+ * line path (3D lattices beyond one CTA, wtd_path3d.cuh): per half step k3_plane_h (when H is
+ * formed), k3_xline, and k3_plane_dens on gradient half steps; then the slot reduction, tau,
+ * the functional and the coefficients as the fused path does them.
+ * -------------------------------------------------------------------------------------*/
+#if CODEDIM == 3
+/* compile-time choice of the x-line kernel's cluster size CL, threads per x-line TX and pad of
+ * its H lines: the first candidate that fits one CTA (<= 1024 threads, shared memory): clusters of
+ * 16 CTAs before 8, teams of line_team(NX) threads before 2 and 1, a pad of 4 before 1 */
+template <typename TC, int CL, int TX, int HPAD> struct LineFit {
+    static constexpr bool ok = TX >= 1 && XSmem<TC, CL, TX, HPAD>::ok && XSmem<TC, CL, TX, HPAD>::bytes + 64 <= WTD_SMEM_MAX;
+};
+template <typename TC> struct LineCfg {
+    static constexpr int T0 = line_team(NX), T1 = T0 > 2 ? 2 : 1;
+#define WTD_LC(cl, tx, hp) LineFit<TC, cl, tx, hp>::ok
+    static constexpr int k =
+        WTD_LC(16, T0, 4) ? 0 : WTD_LC(16, T0, 1) ? 1 : WTD_LC(8, T0, 4) ? 2 : WTD_LC(8, T0, 1) ? 3 :
+        WTD_LC(16, T1, 4) ? 4 : WTD_LC(16, T1, 1) ? 5 : WTD_LC(8, T1, 4) ? 6 : WTD_LC(8, T1, 1) ? 7 :
+        WTD_LC(16, 1, 4) ? 8 : WTD_LC(16, 1, 1) ? 9 : WTD_LC(8, 1, 4) ? 10 : WTD_LC(8, 1, 1) ? 11 : 12;
+#undef WTD_LC
+    static constexpr int CL = (k % 4 < 2) ? 16 : 8;
+    static constexpr int TX = k < 4 ? T0 : k < 8 ? T1 : 1;
+    static constexpr int HPAD = (k % 2 == 0) ? 4 : 1;
+    static constexpr bool ok = k < 12 && PlaneGeo::ok && PlaneSmem<TC>::h_bytes <= WTD_SMEM_MAX &&
+                               PlaneSmem<TC>::d_bytes <= WTD_SMEM_MAX;
+};
+
+static bool line_fits(int prec)
+{
+    if (!WTD_BIG) return false;
+    return prec == WTD_FP64 ? LineCfg<double>::ok : LineCfg<float>::ok;
+}
+
+/* the x-line kernel's attributes (shared memory beyond 48 KB; clusters of 16 CTAs) */
+template <typename TY, typename TH, typename TC, int PASS, bool GRAD>
+static cudaError_t line_x_attrs()
+{
+    typedef LineCfg<TC> L;
+    typedef XSmem<TC, L::CL, L::TX, L::HPAD> SM;
+    auto k = k3_xline<TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD, L::CL, L::TX, L::HPAD>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::bytes);
+    if (e == cudaSuccess && L::CL > 8) e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    return e;
+}
+
+/* launch configuration of ncl clusters on the context stream */
+template <typename TC>
+static void line_x_config(wtd_ctx *c, cudaLaunchConfig_t &cfg, cudaLaunchAttribute *at, int ncl)
+{
+    typedef LineCfg<TC> L;
+    typedef XSmem<TC, L::CL, L::TX, L::HPAD> SM;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3((unsigned)(ncl * L::CL));
+    cfg.blockDim = dim3(SM::XT);
+    cfg.dynamicSmemBytes = SM::bytes;
+    cfg.stream = c->st;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = L::CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+}
+
+template <typename TY, typename TH, typename TC, int PASS, bool GRAD>
+static int line_launch_x(wtd_ctx *c, const StepArgs &a)
+{
+    typedef LineCfg<TC> L;
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute at[1];
+    WTD_ONCE_PER_DEVICE(WTD_CU((line_x_attrs<TY, TH, TC, PASS, GRAD>())));
+    line_x_config<TC>(c, cfg, at, c->ncl);
+    X3Args xa;
+    xa.s = a;
+    xa.K = c->kbuf;
+    WTD_CU(cudaLaunchKernelEx(&cfg, k3_xline<TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD, L::CL, L::TX, L::HPAD>, xa,
+                              (const double2 *)c->tw, (const double *)c->ktab));
+    WTD_LAUNCHED(c);
+    return WTD_OK;
+}
+
+template <typename TY, typename TC>
+static int line_launch_h(wtd_ctx *c, const void *y)
+{
+    typedef PlaneSmem<TC> SM;
+    auto k = k3_plane_h<TY, TC, WTD_VAR>;
+    WTD_ONCE_PER_DEVICE(WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::h_bytes)));
+    k<<<c->p1grid, PlaneGeo::PT, SM::h_bytes, c->st>>>((const TY *)y, (typename cplx<TC>::t *)c->kbuf, c->cf, c->S, c->tw,
+                                                        c->ktab);
+    WTD_LAUNCHED(c);
+    return WTD_OK;
+}
+
+template <typename TY, typename TC>
+static int line_launch_dens(wtd_ctx *c, const void *y)
+{
+    typedef PlaneSmem<TC> SM;
+    constexpr size_t N = WTD_NUMEL;
+    auto k = k3_plane_dens<TY, TC>;
+    WTD_ONCE_PER_DEVICE(WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::d_bytes)));
+    k<<<2 * NX * c->g2, PlaneGeo::PT, SM::d_bytes, c->st>>>((const TY *)y, c->occ, c->wcnt, c->S, c->g2,
+                                                             c->dslot + (size_t)c->ncl * 12 * N, 12 * N, c->tw, c->ktab);
+    WTD_LAUNCHED(c);
+    return WTD_OK;
+}
+
+template <typename TY, typename TH, typename TC, int PASS, bool GRAD>
+static int line_pass_t(wtd_ctx *c, const StepArgs &a)
+{
+    const bool haveH = PASS == 1 || PASS == 3 || (PASS == 0 && !a.fk_given);
+    if (haveH) WTD_TRY((line_launch_h<TY, TC>(c, a.y)));
+    WTD_TRY((line_launch_x<TY, TH, TC, PASS, GRAD>(c, a)));
+    if (GRAD && PASS != 3) WTD_TRY((line_launch_dens<TY, TC>(c, a.yout ? a.yout : a.y)));
+    return WTD_OK;
+}
+
+template <int PASS, bool GRAD>
+static int line_pass_p(wtd_ctx *c, const StepArgs &a)
+{
+    if (c->prec == WTD_FP64) return line_pass_t<double2, double2, double, PASS, GRAD>(c, a);
+    if (c->prec == WTD_MIXED_H64) return line_pass_t<float2, double2, float, PASS, GRAD>(c, a);
+    return line_pass_t<float2, float2, float, PASS, GRAD>(c, a);
+}
+
+/* one half step's kernels (pass 0: H y_k + predictor, 1: H y_pred + corrector, 2: initial
+ * measurement, 3: f_k only), timed like the fused passes when timing is on */
+static int line_pass(wtd_ctx *c, int pass, bool grad, const StepArgs *given)
+{
+    StepArgs a = given ? *given : make_args(c);
+    a.sstride = 12 * WTD_NUMEL;
+    const bool timed = c->timing && pass < 2 && c->nev[pass] < 4096;
+    if (timed) cudaEventRecord(c->ev[pass][0][c->nev[pass]], c->st);
+    int r;
+    if (pass == 0) r = grad ? line_pass_p<0, true>(c, a) : line_pass_p<0, false>(c, a);
+    else if (pass == 1) r = grad ? line_pass_p<1, true>(c, a) : line_pass_p<1, false>(c, a);
+    else if (pass == 2) r = line_pass_p<2, true>(c, a);
+    else r = line_pass_p<3, false>(c, a);
+    if (timed) {
+        cudaEventRecord(c->ev[pass][1][c->nev[pass]], c->st);
+        c->nev[pass]++;
+    }
+    return r;
+}
+
+/* slots -> densities (x-line slots, plus the plane slots on gradient passes), exchange, tau,
+ * potentials and coefficients at time index it (it < 0: none) */
+static int line_after(wtd_ctx *c, bool full, int it)
+{
+    constexpr int N = WTD_NUMEL;
+    const int nslots = c->ncl + (full ? c->g2 : 0);
+    wtd_dens_reduce<<<(12 * N + 255) / 256, 256, 0, c->st>>>(c->dslot, nslots, c->dens, N, full ? 1 : 0, 1.0 / WTD_LPERP,
+                                                             12 * (size_t)N, 12 * N);
+    WTD_LAUNCHED(c);
+    WTD_TRY(exchange(c, c->dens, 12 * (size_t)N));
+    if (full) WTD_TRY(big_tau(c->dens, c->stage3d, c->tw, c->ktab, c->st));
+    if (it < 0) return WTD_OK;
+    WTD_TRY(functional(c, it));
+    return coef_with_friction(c, it);
+}
+
+static int line_step(wtd_ctx *c, bool last)
+{
+    const bool var = WTD_VAR;
+    if (!c->fk_given && !c->have_coef) return WTD_ERR_STATE;
+    c->qfsw = 0.0;
+    WTD_TRY(line_pass(c, 0, var));
+    WTD_TRY(line_after(c, var, c->it + 1));
+    const bool g = var || last;
+    WTD_TRY(line_pass(c, 1, g));
+    WTD_TRY(line_after(c, g, c->it + 1));
+    c->head = (c->head + WTD_NHIST - 1) % WTD_NHIST;
+    c->fk_given = 0;
+    c->it++;
+    return WTD_OK;
+}
+
+static int line_initial(wtd_ctx *c)
+{
+    WTD_TRY(line_pass(c, 2, true));
+    return line_after(c, true, -1);
+}
+
+/* grid sizes of the line kernels on this device */
+template <typename TY, typename TH, typename TC>
+static int line_setup_t(wtd_ctx *c, int nsm)
+{
+    typedef LineCfg<TC> L;
+    int per = 0;
+    {
+        typedef PlaneSmem<TC> SM;
+        auto k = k3_plane_h<TY, TC, WTD_VAR>;
+        WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::h_bytes));
+        WTD_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, PlaneGeo::PT, SM::h_bytes));
+        c->p1grid = nsm * (per > 0 ? per : 1);
+        auto kd = k3_plane_dens<TY, TC>;
+        WTD_CU(cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::d_bytes));
+        WTD_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kd, PlaneGeo::PT, SM::d_bytes));
+        int g = nsm * (per > 0 ? per : 1) / (2 * NX);
+        c->g2 = g < 1 ? 1 : (g > c->S ? c->S : g);
+    }
+    {
+        cudaLaunchConfig_t cfg;
+        cudaLaunchAttribute at[1];
+        WTD_CU((line_x_attrs<TY, TH, TC, 0, false>()));
+        line_x_config<TC>(c, cfg, at, 1);
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, k3_xline<TY, TH, TC, WTD_NHIST, 0, WTD_VAR, false, L::CL, L::TX, L::HPAD>,
+                                           &cfg) != cudaSuccess || ncl < 1) {
+            cudaGetLastError();
+            ncl = nsm / L::CL;
+        }
+        if (ncl < 1) ncl = 1;
+        if (ncl > c->S) ncl = c->S;
+        c->ncl = ncl;
+    }
+    return WTD_OK;
+}
+
+static int line_setup(wtd_ctx *c, int nsm)
+{
+    if (c->prec == WTD_FP64) return line_setup_t<double2, double2, double>(c, nsm);
+    if (c->prec == WTD_MIXED_H64) return line_setup_t<float2, double2, float>(c, nsm);
+    return line_setup_t<float2, float2, float>(c, nsm);
+}
+#else
+static bool line_fits(int) { return false; }
+static int line_pass(wtd_ctx *, int, bool, const StepArgs *) { return WTD_ERR_UNSUPPORTED; }
+static int line_step(wtd_ctx *, bool) { return WTD_ERR_UNSUPPORTED; }
+static int line_initial(wtd_ctx *) { return WTD_ERR_UNSUPPORTED; }
+static int line_setup(wtd_ctx *, int) { return WTD_ERR_UNSUPPORTED; }
+#endif
+
 /* what the adjoint's reverse sweep needs of one fused step */
 struct StepRecord {
     double2 *yk, *yp;           /* state before the step, normalised predictor state */
@@ -669,10 +915,20 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
         const char *pf = getenv("WTD_PREFETCH");
         if (pf) c->prefetch = atoi(pf) & 15;
     }
-    c->staged = WTD_BIG ? 1 : 0;
-    /* plane/pencil lattices: FP64, or complex64 states with FP64 history and arithmetic */
+    /* lattices beyond one CTA.  The FP32-mixed forms take the 3D line path (FP32 arithmetic,
+     * complex64 history possible); FP64 takes the staged path, which measures faster in FP64
+     * on 32^3.  WTD_3D_PATH=line or =staged selects either for every form. */
+    {
+        const char *pp = getenv("WTD_3D_PATH");
+        bool want_line = precision != WTD_FP64;
+        if (pp && strcmp(pp, "line") == 0) want_line = true;
+        if (pp && strcmp(pp, "staged") == 0) want_line = false;
+        c->line = (WTD_BIG && line_fits(precision) && want_line) ? 1 : 0;
+    }
+    c->staged = (WTD_BIG && !c->line) ? 1 : 0;
     if (c->staged && precision == WTD_MIXED_H32) { free(c); return WTD_ERR_UNSUPPORTED; }
-    int per_sm = c->staged ? 2 : occupancy_per_sm(c);
+    if (c->line && line_setup(c, nsm) != WTD_OK) { free(c); return WTD_ERR_CUDA; }
+    int per_sm = WTD_BIG ? 2 : occupancy_per_sm(c);
     c->grid = nsm * per_sm;
     if (c->grid > nwf) c->grid = nwf;
     cudaError_t e = cudaSuccess;
@@ -683,7 +939,13 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     ALLOC(c->occ, nwf * sizeof(double));
     ALLOC(c->kp2, nwf * sizeof(double));
     ALLOC(c->wcnt, nwf * sizeof(double));
-    ALLOC(c->dslot, (size_t)c->grid * 16 * N * sizeof(double)); /* 12 N words, 16 N with quantum friction */
+    {
+        /* density slots: per CTA of the fused passes (12 N words, 16 N with quantum friction);
+         * on the line path per cluster and per plane chunk (12 N words) */
+        size_t slots = (size_t)c->grid * 16 * N;
+        if (c->line && (size_t)(c->ncl + c->g2) * 12 * N > slots) slots = (size_t)(c->ncl + c->g2) * 12 * N;
+        ALLOC(c->dslot, slots * sizeof(double));
+    }
     ALLOC(c->qpe, nwf * sizeof(double));
     ALLOC(c->dens, 16 * N * sizeof(double));
     ALLOC(c->qfld, 4 * N * sizeof(double));
@@ -693,7 +955,14 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     ALLOC(c->eout, 16 * sizeof(double));
     ALLOC(c->tw, WG::twtotal * sizeof(double2));
     ALLOC(c->ktab, 6 * WTD_KT * sizeof(double));
-    if (precision != WTD_FP64) ALLOC(c->stage, n2 * sizeof(double2));
+    if (precision != WTD_FP64) {
+        ALLOC(c->xfer, WTD_XFER * sizeof(double2));
+        if (c->staged) ALLOC(c->stage, n2 * sizeof(double2));
+    }
+    if (c->line) {
+        ALLOC(c->kbuf, n2 * (precision == WTD_FP64 ? sizeof(double2) : sizeof(float2)));
+        ALLOC(c->stage3d, 2 * N * sizeof(double2));
+    }
     if (c->staged) {
         ALLOC(c->ddx, n2 * sizeof(double2));
         ALLOC(c->ddy, n2 * sizeof(double2));
@@ -748,7 +1017,8 @@ int wtd_destroy(wtd_ctx *c)
             for (int k = 0; k < 2; k++)
                 for (int i = 0; i < 4096; i++) cudaEventDestroy(c->ev[p][k][i]);
     void *ptrs[] = {c->y, c->cf, c->occ, c->kp2, c->wcnt, c->dslot, c->qpe, c->dens, c->pots, c->qfld, c->dqf, c->ework,
-                    c->eout, c->tw, c->ktab, c->stage, c->extra, c->ddx, c->ddy, c->ddz, c->dlap, c->dalap, c->stage3d};
+                    c->eout, c->tw, c->ktab, c->stage, c->extra, c->ddx, c->ddy, c->ddz, c->dlap, c->dalap, c->stage3d,
+                    c->kbuf, c->xfer};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) if (ptrs[i]) cudaFree(ptrs[i]);
     for (int h = 0; h < WTD_NHIST; h++) if (c->hist[h]) cudaFree(c->hist[h]);
     if (c->st) cudaStreamDestroy(c->st);
@@ -816,15 +1086,20 @@ int wtd_process_params(wtd_ctx *c, double *params, double *kF, double *mu)
     return WTD_OK;
 }
 
+/* complex64 arrays go through the bounded staging buffer in chunks of WTD_XFER complex
+ * numbers (host FP64 <-> device complex64), in stream order */
 static int upload_array(wtd_ctx *c, void *dst, int prec_elem64, const double *host)
 {
     const size_t n2 = (size_t)2 * c->S * WTD_NUMEL;
     if (prec_elem64) {
         WTD_CU(cudaMemcpyAsync(dst, host, n2 * sizeof(double2), cudaMemcpyHostToDevice, c->st));
     } else {
-        WTD_CU(cudaMemcpyAsync(c->stage, host, n2 * sizeof(double2), cudaMemcpyHostToDevice, c->st));
-        wtd_convert_in<float2><<<(unsigned)((n2 + 255) / 256), 256, 0, c->st>>>(c->stage, (float2 *)dst, n2);
-        WTD_LAUNCHED(c);
+        for (size_t o = 0; o < n2; o += WTD_XFER) {
+            const size_t m = n2 - o < WTD_XFER ? n2 - o : WTD_XFER;
+            WTD_CU(cudaMemcpyAsync(c->xfer, host + 2 * o, m * sizeof(double2), cudaMemcpyHostToDevice, c->st));
+            wtd_convert_in<float2><<<(unsigned)((m + 255) / 256), 256, 0, c->st>>>((const double2 *)c->xfer, (float2 *)dst + o, m);
+            WTD_LAUNCHED(c);
+        }
     }
     return WTD_OK;
 }
@@ -834,9 +1109,12 @@ static int download_array(wtd_ctx *c, const void *src, int prec_elem64, double *
     if (prec_elem64) {
         WTD_CU(cudaMemcpyAsync(host, src, n2 * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
     } else {
-        wtd_convert_out<float2><<<(unsigned)((n2 + 255) / 256), 256, 0, c->st>>>((const float2 *)src, c->stage, n2);
-        WTD_LAUNCHED(c);
-        WTD_CU(cudaMemcpyAsync(host, c->stage, n2 * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+        for (size_t o = 0; o < n2; o += WTD_XFER) {
+            const size_t m = n2 - o < WTD_XFER ? n2 - o : WTD_XFER;
+            wtd_convert_out<float2><<<(unsigned)((m + 255) / 256), 256, 0, c->st>>>((const float2 *)src + o, (double2 *)c->xfer, m);
+            WTD_LAUNCHED(c);
+            WTD_CU(cudaMemcpyAsync(host + 2 * o, c->xfer, m * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+        }
     }
     WTD_CU(cudaStreamSynchronize(c->st));
     return WTD_OK;
@@ -932,6 +1210,10 @@ int wtd_initial_measurement(wtd_ctx *c, int it0)
         WTD_TRY(staged_initial(c));
         return wtd_cuerr(cudaGetLastError());
     }
+    if (c->line) {
+        WTD_TRY(line_initial(c));
+        return wtd_cuerr(cudaGetLastError());
+    }
     WTD_TRY(run_pass(c, 2, true));
     WTD_TRY(after_pass(c, true, -1));
     return wtd_cuerr(cudaGetLastError());
@@ -944,6 +1226,10 @@ int wtd_steps(wtd_ctx *c, int nsteps)
     const bool var = WTD_VAR;
     if (c->staged) {
         for (int s = 0; s < nsteps; s++) WTD_TRY(staged_step(c, s == nsteps - 1));
+        return WTD_OK;
+    }
+    if (c->line) {
+        for (int s = 0; s < nsteps; s++) WTD_TRY(line_step(c, s == nsteps - 1));
         return WTD_OK;
     }
     (void)var;
@@ -1083,6 +1369,21 @@ int wtd_set_quantum_friction(wtd_ctx *c, double alpha, double beta, double gamma
     if (!c) return WTD_ERR_ARG;
     const bool on = alpha != 0.0 || beta != 0.0 || gamma != 0.0;
     if (on && !(ramp > 0.0)) return WTD_ERR_ARG;
+    if (on && c->line) {
+        /* the line path has no friction densities: the run continues on the staged path, which
+         * keeps the same state, ring and f_k conventions (FP64 only) */
+        if (c->prec != WTD_FP64) return WTD_ERR_UNSUPPORTED;
+        WTD_CU(cudaSetDevice(c->dev));
+        if (!c->fk_given && c->have_coef) WTD_TRY(ensure_fk(c));
+        const size_t n2 = (size_t)2 * c->S * WTD_NUMEL;
+        cudaError_t e = cudaSuccess;
+        double2 **bufs[5] = {&c->ddx, &c->ddy, &c->ddz, &c->dlap, &c->dalap};
+        for (int k = 0; k < 5 && e == cudaSuccess; k++)
+            if ((k < 4 || WTD_VAR) && !*bufs[k]) e = cudaMalloc((void **)bufs[k], n2 * sizeof(double2));
+        if (e != cudaSuccess) { cudaGetLastError(); return WTD_ERR_NOMEM; }
+        c->line = 0;
+        c->staged = 1;
+    }
     c->qf[0] = alpha; c->qf[1] = beta; c->qf[2] = gamma; c->qf[3] = nreq;
     c->qf[4] = start; c->qf[5] = stop; c->qf[6] = ramp;
     c->sstride = (on ? 16 : 12) * WTD_NUMEL;

@@ -191,6 +191,8 @@ extern "C" int wtd_checkpoint_load(wtd_ctx *c, const char *dir, int rank, int nr
     c->fk_given = 1;
     if (c->staged) {
         WTD_TRY(staged_initial(c));
+    } else if (c->line) {
+        WTD_TRY(line_initial(c));
     } else {
         WTD_TRY(run_pass(c, 2, true));
         WTD_TRY(after_pass(c, true, -1));

@@ -12,8 +12,7 @@
  *   [S', S'+18N)      per-point H coefficients (the CF_* list)
  *   [.., +G*12N)      density partial sums of the G CTAs of calculate_densities
  *   [.., +2S')        per-state |k_perp|^2 and degeneracy weights of the plane-wave factor
- *   [.., +2N)         scratch of compute_divergence_real_vector_f
- * so the per-step calls of a driver that sized and set the work area allocate nothing.
+ * so calculate_densities and apply_hamiltonian allocate nothing once the work area is set.
  */
 #ifndef WTD_COMPAT_CUH
 #define WTD_COMPAT_CUH
@@ -29,11 +28,9 @@ static double *compat_qpe(void) { return (double *)g_work; }
 static double *compat_cf(void) { return (double *)g_work + compat_spad(); }
 static double *compat_slots(void) { return (double *)g_work + compat_spad() + (size_t)CF_COUNT * WTD_NUMEL; }
 static double *compat_kpw(void) { return compat_slots() + (size_t)g_dens_grid * 12 * WTD_NUMEL; }
-static double *compat_divtmp(void) { return compat_kpw() + 2 * compat_spad(); }
 static size_t compat_work_words(void)
 {
-    return compat_spad() + (size_t)CF_COUNT * WTD_NUMEL + (size_t)g_dens_grid * 12 * WTD_NUMEL + 2 * compat_spad() +
-           2 * (size_t)WTD_NUMEL;
+    return compat_spad() + (size_t)CF_COUNT * WTD_NUMEL + (size_t)g_dens_grid * 12 * WTD_NUMEL + 2 * compat_spad();
 }
 
 static int cu_sync_status(void)
@@ -518,15 +515,16 @@ __global__ void k_planewave(int n, const double *kky, const double *kkz, const i
 #endif
 }
 
-/* the per-state plane-wave arrays of the current call: in the work area when it is set and
- * sized for n states; otherwise (calculate_quantum_friction_densities before the work area is
- * set) in a library-owned pair that is allocated when it first has to grow */
+/* the per-state plane-wave arrays of the current call: in the work area for the calls that
+ * require it anyway (calculate_densities, apply_hamiltonian: in_work); otherwise
+ * (calculate_quantum_friction_densities, which needs no work area) in a library-owned pair that
+ * is allocated when it first has to grow */
 static double *g_kp2 = NULL, *g_wcnt = NULL;
 static double *g_kp2_own = NULL, *g_wcnt_own = NULL;
 static int g_kp_own_n = 0;
-static int compat_planewave(int n, const double *kky, const double *kkz, const int *cnt)
+static int compat_planewave(int n, const double *kky, const double *kkz, const int *cnt, bool in_work)
 {
-    if (g_work && n <= g_nwfip) {
+    if (in_work && g_work && n <= g_nwfip) {
         g_kp2 = compat_kpw();
         g_wcnt = g_kp2 + compat_spad();
     } else {
@@ -799,21 +797,16 @@ int compute_derivative_real_vector_f(double *fx, double *fy, double *fz, double 
     if (!r && CODEDIM >= 3 && fz) r = compat_real_deriv(fz, dfz_dz, 3);
     return r;
 }
-/* scratch of the divergence: the work area's 2 N words, or (work area not yet set) a
- * library-owned array allocated on the first such call and kept */
+/* scratch of the divergence: a library-owned array of 2 N words, allocated on the first such
+ * call and kept (the call needs no work area, so it must not depend on one being alive) */
 static double *g_divtmp_own = NULL;
 int compute_divergence_real_vector_f(double *fx, double *fy, double *fz, double *divf, int nthreads)
 {
-    double *t = NULL;
-    if (g_work) {
-        t = compat_divtmp();
-    } else {
-        if (!g_divtmp_own && cudaMalloc((void **)&g_divtmp_own, 2 * sizeof(double) * WTD_NUMEL) != cudaSuccess) {
-            g_divtmp_own = NULL;
-            return WTD_ERR_NOMEM;
-        }
-        t = g_divtmp_own;
+    if (!g_divtmp_own && cudaMalloc((void **)&g_divtmp_own, 2 * sizeof(double) * WTD_NUMEL) != cudaSuccess) {
+        g_divtmp_own = NULL;
+        return WTD_ERR_NOMEM;
     }
+    double *t = g_divtmp_own;
     int r = compat_real_deriv(fx, divf, 1);
     if (!r && CODEDIM >= 2) { r = compat_real_deriv(fy, t, 2); }
     if (!r && CODEDIM >= 3) { r = compat_real_deriv(fz, t + WTD_NUMEL, 3); }
@@ -867,7 +860,7 @@ static int calculate_densities_impl(int n, wtd_z *wf, wtd_z *dx, wtd_z *dy, wtd_
                                     const double *kkz, const int *cnt, double *fb, double *w, double *dens, int grads)
 {
     if (!g_work || g_nwfip < n || g_dens_grid <= 0) return WTD_ERR_STATE;
-    int r = compat_planewave(n, kky, kkz, cnt);
+    int r = compat_planewave(n, kky, kkz, cnt, true);
     if (r) return r;
     double *slots = compat_slots();
     int G = g_dens_grid < n ? g_dens_grid : n;
@@ -991,7 +984,7 @@ static int apply_hamiltonian_impl(int it, int n, wtd_z *in, wtd_z *out, wtd_z *d
 #endif
     int r = compat_coefficients(it, pots, fld == pots ? NULL : fld);
     if (r) return r;
-    r = compat_planewave(n, kky, kkz, NULL);
+    r = compat_planewave(n, kky, kkz, NULL, true);
     if (r) return r;
     k_hamiltonian_compat<<<n, 256>>>(n, (const double2 *)in, (double2 *)out, (const double2 *)dx, (const double2 *)dy,
                                      (const double2 *)dz, (const double2 *)lap, (const double2 *)alap, compat_cf(), g_kp2,
@@ -1032,7 +1025,7 @@ static int calculate_qf_densities_impl(int n, const wtd_z *wf, const wtd_z *lap,
                                 const int *cnt, const double *fb, const double *w, double *qf)
 {
     if (n <= 0 || !wf || !lap || !fb || !qf) return WTD_ERR_ARG;
-    int r = compat_planewave(n, kky, kkz, cnt);
+    int r = compat_planewave(n, kky, kkz, cnt, false);
     if (r) return r;
     k_qf_dens_compat<<<(WTD_NUMEL + 255) / 256, 256>>>(n, (const double2 *)wf, (const double2 *)lap, fb, w, g_kp2, g_wcnt,
                                                        qf, 1.0 / WTD_LPERP);

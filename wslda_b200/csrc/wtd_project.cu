@@ -16,6 +16,7 @@
 #include "wtd_functional.cuh"
 #include "wtd_lattice.cuh"
 #include "wtd_fft3d.cuh"
+#include "wtd_path3d.cuh"
 #define WTD_CODEDIM CODEDIM
 #include "wtd_compat.cuh"
 #include "wtd_api.cuh"
