@@ -10,10 +10,13 @@ density reductions and both functional evaluations).
 Arms:
   wtd        this library (libwtd.so through its C ABI); prints one JSON line with value
              (device-timed, inputs resident), e2e (host buffers through the public API),
-             roofline of the dominant kernel, cpu_baseline (oracle port on host cores),
-             the FP32-mixed forms and the reference's own CUDA kernels on the same GPU.
-  reference  the reference's step on the host cores (the CPU oracle port, all threads), on a
-             bounded sample of the same workload.
+             roofline of the dominant kernel, cpu_baseline (the host-core baseline below),
+             the FP32-mixed forms, the reference's own CUDA kernels on the same GPU and inputs,
+             the 3D comparisons (C3, C5) and the adjoint's cost (C4).
+  reference  the step on the host cores with all threads, on a bounded sample of the same
+             workload: the state derivatives from the reference's lib/wderiv (compiled
+             unmodified over an FFTW-API shim) plus the oracle's local update; the oracle port
+             alone where that build is absent.
 Multi-GPU (torchrun): the workload's states are sharded over ranks in contiguous blocks (strong
 scaling: one physical system of a fixed state count); after every density reduction NCCL sums
 the partial densities over ranks on the context stream (the step's one exchange), and the
@@ -302,8 +305,12 @@ def time_adjoint(r, proj, d, stream, steps=0):
     for label, k in (("auto", 0), (f"K{K}", K)):
         t_first = timed(nparam=npar, checkpoint_every=k)[0]
         tg, loss_g, g = timed(nparam=npar, checkpoint_every=k)
+        # the call split at the loss: the forward with its checkpoints, and the reverse sweep
+        # (segment recomputation and adjoint steps) — the adjoint proper
+        ms_fwd, ms_rev = r.adjoint_times()
         out[label] = {"checkpoint_every": k or "auto", "ms_gradient": tg, "ms_first_call": t_first,
-                      "gradient_over_forward": tg / tf}
+                      "gradient_over_forward": tg / tf, "ms_forward_in_call": ms_fwd, "ms_reverse_sweep": ms_rev,
+                      "adjoint_over_forward": ms_rev / tf}
         r.adjoint_release()
     out["loss"] = loss
     out["grad_norm"] = float(np.linalg.norm(g))
@@ -565,6 +572,36 @@ def adjoint_c4(args, dev):
     return out
 
 
+def probe(args):
+    """one form of one workload on one GPU: device time of --steps steps after the initial
+    measurement and --warmup steps (the case the ncu captures of the line path run)"""
+    import torch
+    from wslda_b200 import TDRun
+    wl = WORKLOADS[args.workload]
+    nwf = args.nwf or wl["nwf"]
+    proj, d = make_inputs(wl["project"], nwf)
+    r = TDRun(wl["project"], nwf, precision=args.probe, device=0)
+    r.setup(d["states"], d["pots"], d["occ"], d["params"], d["extra"])
+    r.initial_measurement()
+    r.steps(args.warmup)
+    r.sync()
+    stream = torch.cuda.ExternalStream(r.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    l0 = r.launches()
+    e0.record(stream)
+    r.steps(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out = {"probe": wl["project"], "states": nwf, "precision": args.probe, "steps": args.steps,
+           "path_3d": os.environ.get("WTD_3D_PATH", "default"), "ms_per_step": ms / args.steps,
+           "value": nwf * args.steps / (ms * 1e-3), "unit": "qp-state*steps/s",
+           "launches_per_step": (r.launches() - l0) / args.steps}
+    r.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -593,6 +630,9 @@ def main():
     ap.add_argument("--c5-steps", type=int, default=3)
     ap.add_argument("--c5-err-nwf", type=int, default=256)
     ap.add_argument("--c5-err-steps", type=int, default=20)
+    ap.add_argument("--probe", type=int, default=-1, choices=[-1, 0, 1, 2],
+                    help="time one precision form (0 FP64, 1 mixed H64, 2 mixed H32) of the workload for --steps "
+                         "steps after --warmup, print one short JSON line and exit (the profiling case)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     args.blocks = max(args.blocks, 1)
@@ -625,6 +665,10 @@ def main():
                         "(lib/wderiv) and the oracle's restatement of the rest of the step",
                 "wall_s": round(time.perf_counter() - t0, 1)}
         print(json.dumps(line))
+        return
+
+    if args.probe >= 0:
+        print(json.dumps(probe(args)))
         return
 
     if world > 1:

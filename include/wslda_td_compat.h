@@ -58,6 +58,29 @@ void *mm_get_pointer_to_kernels_workspace(size_t n);
 void *mm_get_pointer_to_derivatives_workspace(size_t n);
 void *mm_get_pointer_to_total_workspace(size_t n);
 
+/* host forms of the energy-density-functional pieces (hpc-engine/pca_kernels.h:11-30,
+ * cpca_kernels.h, ccpca_kernels.h; pca_edf.h:46-350), called by the drivers' uniform-solution
+ * start (pca_uniform.h) */
+double polarization_h(double n_a, double n_b);
+double der_polarization__der_na_h(double n_a, double n_b);
+double der_polarization__der_nb_h(double n_a, double n_b);
+double alpha_h(double p);
+double alpha_a_h(double p);
+double alpha_b_h(double p);
+double alpha_plus_h(double p);
+double alpha_minus_h(double p);
+double der_alpha_plus__der_na_h(double n_a, double n_b);
+double der_alpha_plus__der_nb_h(double n_a, double n_b);
+double der_alpha_minus__der_na_h(double n_a, double n_b);
+double der_alpha_minus__der_nb_h(double n_a, double n_b);
+double funG_h(double p);
+double funD_h(double n_a, double n_b);
+double der_funD__der_na_h(double n_a, double n_b);
+double der_funD__der_nb_h(double n_a, double n_b);
+double tildeC_h(double n_a, double n_b);
+double der_tildeC__der_na_h(double n_a, double n_b);
+double der_tildeC__der_nb_h(double n_a, double n_b);
+
 /* ABM predictor / corrector (hpc-engine/tdwslda_ode_integrator.h:106, :195) */
 int abm_step1(int n, wtd_z *ykm1, wtd_z *fkm1, wtd_z *fkm2, wtd_z *fkm3, wtd_z *fkm4, wtd_z *fkm5,
               int abm_scheme, int nthreads);

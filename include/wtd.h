@@ -172,6 +172,18 @@ int wtd_pass_times(wtd_ctx *ctx, double *ms_pass_a, double *ms_pass_b, int *coun
 int wtd_adjoint(wtd_ctx *ctx, int it0, int nsteps, int checkpoint_every, const double *mask, int nparam,
                 double *loss, double *grad);
 int wtd_adjoint_release(wtd_ctx *ctx);
+/* The same in two calls, for callers with a separate backward (an autograd function):
+ * wtd_adjoint_forward runs the forward of wtd_adjoint with its checkpoints and records and
+ * returns L; wtd_adjoint_backward then runs the reverse sweep and returns dL/dparams[0..nparam).
+ * Between the two the context must not change: any launch, upload or setter on it makes the
+ * backward return WTD_ERR_STATE (so does a backward without a forward).  After the backward the
+ * context is again where the forward left it, and a second backward may follow. */
+int wtd_adjoint_forward(wtd_ctx *ctx, int it0, int nsteps, int checkpoint_every, const double *mask, double *loss);
+int wtd_adjoint_backward(wtd_ctx *ctx, int nparam, double *grad);
+/* device time of the last adjoint forward (initial measurement, nsteps steps with checkpoints
+ * and records, the loss) and of the last reverse sweep after it (recomputed segments and the
+ * adjoint steps; 0 if none); WTD_ERR_STATE before any adjoint call */
+int wtd_adjoint_times(wtd_ctx *ctx, double *ms_forward, double *ms_reverse);
 
 /* high-k filters of the fields H is built from, f -> IFFT[FD(k^2/2; mu, T) FFT f], in place
  * after every functional evaluation, as the reference's driver and apply_hamiltonian do

@@ -2,9 +2,11 @@
 
 StirrerLoss.apply(theta, run, inp, nsteps, mask, checkpoint_every) runs the forward of a TDRun
 from the seeded start state with the first len(theta) user parameters set to theta and returns
-the loss L = sum_r |Delta(r, T)|^2 mask(r) dV as a 0-d float64 tensor.  Its backward returns
-grad_output * dL/dtheta from the library's reverse sweep (wtd_adjoint: checkpointed forward,
-segment recompute, adjoint ABM steps), so the loss composes with any torch expression.
+the loss L = sum_r |Delta(r, T)|^2 mask(r) dV as a 0-d float64 tensor.  The forward is the
+library's recorded forward (wtd_adjoint_forward: checkpoints every checkpoint_every steps);
+the backward is its reverse sweep (wtd_adjoint_backward: segment recompute, adjoint ABM steps)
+and returns grad_output * dL/dtheta, so the loss composes with any torch expression.  The run
+must not be used between the two.
 """
 import numpy as np
 import torch
@@ -17,13 +19,14 @@ class StirrerLoss(torch.autograd.Function):
         th = theta.detach().cpu().numpy().astype(np.float64)
         params[: th.size] = th
         run.setup(inp["states"], inp["pots"], inp["occ"], params, inp["extra"])
-        need = ctx.needs_input_grad[0]
-        loss, grad = run.adjoint(nsteps, nparam=th.size if need else 0, mask=mask, checkpoint_every=checkpoint_every)
-        if need:
-            ctx.save_for_backward(torch.from_numpy(grad).to(theta.dtype))
+        if ctx.needs_input_grad[0]:
+            loss = run.adjoint_forward(nsteps, mask=mask, checkpoint_every=checkpoint_every)
+        else:
+            loss, _ = run.adjoint(nsteps, mask=mask)
+        ctx.run, ctx.nparam, ctx.dtype = run, th.size, theta.dtype
         return torch.tensor(loss, dtype=theta.dtype)
 
     @staticmethod
     def backward(ctx, grad_output):
-        (g,) = ctx.saved_tensors
+        g = torch.from_numpy(ctx.run.adjoint_backward(ctx.nparam)).to(ctx.dtype)
         return grad_output * g, None, None, None, None, None

@@ -134,6 +134,9 @@ def test_adjoint_leaves_forward_state(setup_run):
     run.adjoint(NSTEPS, nparam=NPARAM, checkpoint_every=3)
     assert run.time_index() == it_ref
     assert np.array_equal(run.states(), y_ref)
+    # the call's device time, split at the loss: both parts ran
+    ms_fwd, ms_rev = run.adjoint_times()
+    assert ms_fwd > 0 and ms_rev > 0
 
 
 @pytest.mark.gpu
@@ -204,3 +207,29 @@ def test_adjoint_through_torch_autograd(setup_run):
     torch.log1p(L * L).backward()
     lv = float(L.detach())
     assert rel(theta2.grad.numpy(), 2 * lv / (1 + lv * lv) * g) < 1e-12
+
+
+@pytest.mark.gpu
+def test_adjoint_split_forward_backward(setup_run):
+    """wtd_adjoint_forward + wtd_adjoint_backward give the one-call gradient bit for bit; the
+    backward refuses after the run changed, and a second backward repeats the first"""
+    from wslda_b200 import WtdError
+    proj, d, run, fresh = setup_run
+    m = _mask(proj)
+    fresh(d["params"])
+    loss1, g1 = run.adjoint(NSTEPS, nparam=NPARAM, mask=m, checkpoint_every=3)
+    fresh(d["params"])
+    loss2 = run.adjoint_forward(NSTEPS, mask=m, checkpoint_every=3)
+    g2 = run.adjoint_backward(NPARAM)
+    assert loss1 == loss2 and np.array_equal(g1, g2)
+    assert np.array_equal(run.adjoint_backward(NPARAM), g2)
+    ms_fwd, ms_rev = run.adjoint_times()
+    assert ms_fwd > 0 and ms_rev > 0
+    run.steps(1)
+    with pytest.raises(WtdError):
+        run.adjoint_backward(NPARAM)
+    fresh(d["params"])
+    run.adjoint_forward(NSTEPS, mask=m, checkpoint_every=3)
+    run.upload_states(d["states"])
+    with pytest.raises(WtdError):
+        run.adjoint_backward(NPARAM)

@@ -63,6 +63,9 @@ SIGNATURES = {
     "wtd_pass_times": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _ip, _ip]),
     "wtd_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp]),
     "wtd_adjoint_release": (ctypes.c_int, [ctypes.c_void_p]),
+    "wtd_adjoint_times": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    "wtd_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]),
+    "wtd_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "wtd_set_high_k_filter": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double]),
     "wtd_set_quantum_friction": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_double] * 7),
     "wtd_nccl_unique_id": (ctypes.c_int, [ctypes.c_void_p]),
@@ -283,6 +286,27 @@ class TDRun:
         qfstop, qfswitch (times in 1/eF); all coefficients 0 turns it off"""
         self._check(self.lib.wtd_set_quantum_friction(self.h, *[float(x) for x in (alpha, beta, gamma, nreq, start,
                                                                                    stop, ramp)]))
+
+    def adjoint_forward(self, nsteps, mask=None, checkpoint_every=0, it0=None):
+        """the forward of adjoint() with its checkpoints and records, for a later
+        adjoint_backward(); returns L.  The run must not change before the backward."""
+        loss = np.zeros(1)
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
+        self._check(self.lib.wtd_adjoint_forward(self.h, int(self.it0 if it0 is None else it0), int(nsteps),
+                                                 int(checkpoint_every), _p(m), _p(loss)))
+        return float(loss[0])
+
+    def adjoint_backward(self, nparam):
+        """the reverse sweep after adjoint_forward(): dL/dparams[:nparam]"""
+        grad = np.zeros(nparam)
+        self._check(self.lib.wtd_adjoint_backward(self.h, int(nparam), _p(grad)))
+        return grad
+
+    def adjoint_times(self):
+        """(ms of the last adjoint forward, ms of the reverse sweep after it), device-timed"""
+        a, b = np.zeros(1), np.zeros(1)
+        self._check(self.lib.wtd_adjoint_times(self.h, _p(a), _p(b)))
+        return float(a[0]), float(b[0])
 
     def adjoint_release(self):
         """free the adjoint's device workspace (kept between gradient calls)"""

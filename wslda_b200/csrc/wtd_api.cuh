@@ -37,6 +37,7 @@ struct wtd_ctx {
     double dt;
     cudaStream_t st;
     long long launches;
+    long long mut;              /* uploads and setters so far (a recorded adjoint forward checks it) */
     /* optional device timing of the fused passes: events around each pass, summed on demand */
     int timing;
     cudaEvent_t ev[2][2][4096];
@@ -1029,6 +1030,7 @@ int wtd_destroy(wtd_ctx *c)
 int wtd_set_constants(wtd_ctx *c, double mu_a, double mu_b, double ec, double t0, double dt, double kF)
 {
     if (!c) return WTD_ERR_ARG;
+    c->mut++;
     WTD_CU(cudaSetDevice(c->dev));
     double eF = kF * kF / 2., nF = kF * kF * kF / (3. * M_PI * M_PI);
     WTD_CU(cudaMemcpyToSymbol(dc_mu_a, &mu_a, sizeof(double)));
@@ -1048,6 +1050,7 @@ int wtd_set_constants(wtd_ctx *c, double mu_a, double mu_b, double ec, double t0
 int wtd_set_params(wtd_ctx *c, const double *params)
 {
     if (!c || !params) return WTD_ERR_ARG;
+    c->mut++;
     WTD_CU(cudaSetDevice(c->dev));
     WTD_CU(cudaMemcpyToSymbol(dc_params, params, MAX_USER_PARAMS * sizeof(double)));
     memcpy(md.params, params, MAX_USER_PARAMS * sizeof(double));
@@ -1057,6 +1060,7 @@ int wtd_set_params(wtd_ctx *c, const double *params)
 int wtd_set_sclgth(wtd_ctx *c, double a)
 {
     if (!c) return WTD_ERR_ARG;
+    c->mut++;
     WTD_CU(cudaSetDevice(c->dev));
     WTD_CU(cudaMemcpyToSymbol(dc_sclgth, &a, sizeof(double)));
     hc_sclgth = a;
@@ -1067,6 +1071,7 @@ int wtd_set_sclgth(wtd_ctx *c, double a)
 int wtd_set_extra_data(wtd_ctx *c, const void *host, size_t bytes)
 {
     if (!c || (bytes && !host)) return WTD_ERR_ARG;
+    c->mut++;
     WTD_CU(cudaSetDevice(c->dev));
     if (c->extra) { cudaFree(c->extra); c->extra = NULL; }
     if (bytes) {
@@ -1123,6 +1128,7 @@ static int download_array(wtd_ctx *c, const void *src, int prec_elem64, double *
 int wtd_upload_states(wtd_ctx *c, const double *host)
 {
     if (!c || !host) return WTD_ERR_ARG;
+    c->mut++;
     WTD_CU(cudaSetDevice(c->dev));
     return upload_array(c, c->y, c->prec == WTD_FP64, host);
 }
@@ -1141,6 +1147,7 @@ static int ring_of_ref_slot(int s) { return s == 0 ? WTD_NHIST - 1 : s - 1; }
 int wtd_upload_history(wtd_ctx *c, int slot, const double *host)
 {
     if (!c || !host || slot < 0 || slot >= WTD_NHIST) return WTD_ERR_ARG;
+    c->mut++;
     WTD_CU(cudaSetDevice(c->dev));
     void *s[5];
     ring_slots(c, s);
@@ -1162,6 +1169,7 @@ int wtd_download_history(wtd_ctx *c, int slot, double *host)
 int wtd_upload_potentials(wtd_ctx *c, const double *host)
 {
     if (!c || !host) return WTD_ERR_ARG;
+    c->mut++;
     WTD_CU(cudaSetDevice(c->dev));
     WTD_CU(cudaMemcpyAsync(c->pots, host, 12 * (size_t)WTD_NUMEL * sizeof(double), cudaMemcpyHostToDevice, c->st));
     return WTD_OK;
@@ -1170,6 +1178,7 @@ int wtd_upload_potentials(wtd_ctx *c, const double *host)
 int wtd_upload_occupations(wtd_ctx *c, const double *fbeta, const double *kky, const double *kkz, const int *cnt)
 {
     if (!c || !fbeta) return WTD_ERR_ARG;
+    c->mut++;
     WTD_CU(cudaSetDevice(c->dev));
     const int S = c->S;
     double *kp2 = (double *)malloc(S * sizeof(double)), *w = (double *)malloc(S * sizeof(double));
@@ -1728,7 +1737,24 @@ struct AdjWork {
     std::vector<StepRecord> rec;
     double2 *ybar = NULL, *ypbar = NULL, *pbar = NULL, *fring[WTD_NHIST] = {};
     double *fields = NULL, *dgrad = NULL, *tpart = NULL, *dloss = NULL, *dmask = NULL;
-    explicit AdjWork(cudaStream_t s) : pool(s) {}
+    /* events of the last forward (start, loss) and of the last reverse sweep (start, end) */
+    cudaEvent_t ev[4] = {};
+    bool timed_f = false, timed_r = false;
+    /* a recorded forward the reverse sweep may follow: its schedule, the time index of each
+     * step of the last segment, and the context's counters when it ended (any later launch,
+     * upload or setter invalidates it) */
+    bool ready = false;
+    int K = 0, nsteps = 0, nseg = 0, last0 = 0;
+    std::vector<int> itk;
+    long long mark_launches = 0, mark_mut = 0;
+    explicit AdjWork(cudaStream_t s) : pool(s)
+    {
+        for (auto &e : ev) cudaEventCreate(&e);
+    }
+    ~AdjWork()
+    {
+        for (auto &e : ev) if (e) cudaEventDestroy(e);
+    }
 };
 
 static size_t adj_record_bytes(const wtd_ctx *c)
@@ -1816,37 +1842,38 @@ static int adj_choose_K(wtd_ctx *c, int nsteps, int K)
     return -1;
 }
 
-static int adjoint_run(wtd_ctx *c, int it0, int nsteps, int Kin, const double *mask_h, int nparam, double *loss_h,
-                       double *grad_h)
+/* the forward from the uploaded states: initial measurement(it0), nsteps steps and the loss.
+ * record: keep a checkpoint every K steps and the last segment's step records, so that
+ * adjoint_reverse can follow (K from Kin as adj_choose_K picks it) */
+static int adjoint_forward(wtd_ctx *c, int it0, int nsteps, int Kin, const double *mask_h, bool record, double *loss_h)
 {
-    constexpr int N = WTD_NUMEL, NH = WTD_NHIST;
-    const int S = c->S;
-    const size_t NS = (size_t)2 * S * N;
+    constexpr int N = WTD_NUMEL;
     constexpr size_t sm = 2 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>) +
                           80 * sizeof(double);
     if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
-    const bool grad = grad_h != NULL;
-    const int K = grad ? adj_choose_K(c, nsteps, Kin) : 0;
-    if (grad && K < 1) return WTD_ERR_NOMEM;
-    const int nseg = grad ? (nsteps + K - 1) / K : 1;
+    const int K = record ? adj_choose_K(c, nsteps, Kin) : 0;
+    if (record && K < 1) return WTD_ERR_NOMEM;
+    const int nseg = record ? (nsteps + K - 1) / K : 1;
     const int last0 = (nseg - 1) * K; /* first step of the last segment, recorded by the forward */
     AdjWork *w = NULL;
-    WTD_TRY(adj_workspace(c, K, grad ? nseg - 1 : 0, &w));
-    double *vbar = w->fields;
+    WTD_TRY(adj_workspace(c, K, record ? nseg - 1 : 0, &w));
+    w->ready = false;
+    w->K = K; w->nsteps = nsteps; w->nseg = nseg; w->last0 = last0;
+    w->itk.assign(K > 0 ? K : 1, 0);
     double2 *nubar = (double2 *)(w->fields + 2 * (size_t)N);
     if (mask_h) WTD_CU(cudaMemcpyAsync(w->dmask, mask_h, N * sizeof(double), cudaMemcpyHostToDevice, c->st));
 
-    /* forward from the uploaded states */
-    std::vector<int> itk(K > 0 ? K : 1);
+    w->timed_f = w->timed_r = false;
+    WTD_CU(cudaEventRecord(w->ev[0], c->st));
     WTD_TRY(wtd_initial_measurement(c, it0));
     for (int s = 0; s < nsteps; s++) {
         StepRecord *r = NULL;
-        if (grad && s < last0 && s % K == 0) WTD_TRY(ck_copy(c, true, w->ck[s / K]));
+        if (record && s < last0 && s % K == 0) WTD_TRY(ck_copy(c, true, w->ck[s / K]));
         double2 *next = NULL;
-        if (grad && s >= last0) {
+        if (record && s >= last0) {
             const int j = s - last0;
             r = &w->rec[j];
-            itk[j] = c->it;
+            w->itk[j] = c->it;
             if (j == 0) WTD_CU(cudaMemcpyAsync(r->yk, c->y, c->ysz, cudaMemcpyDeviceToDevice, c->st));
             if (s + 1 < nsteps) next = w->rec[j + 1].yk;
         }
@@ -1855,7 +1882,32 @@ static int adjoint_run(wtd_ctx *c, int it0, int nsteps, int Kin, const double *m
     k_adj_loss<<<1, 512, 0, c->st>>>(c->pots, mask_h ? w->dmask : NULL, nubar, w->dloss);
     WTD_LAUNCHED(c);
     WTD_CU(cudaMemcpyAsync(loss_h, w->dloss, sizeof(double), cudaMemcpyDeviceToHost, c->st));
-    if (!grad) return wtd_cuerr(cudaStreamSynchronize(c->st));
+    WTD_CU(cudaEventRecord(w->ev[1], c->st));
+    WTD_TRY(wtd_cuerr(cudaStreamSynchronize(c->st)));
+    w->timed_f = true;
+    w->ready = record;
+    w->mark_launches = c->launches;
+    w->mark_mut = c->mut;
+    return WTD_OK;
+}
+
+/* the reverse sweep after a recorded forward: dL/dparams[0..nparam) into grad_h; the context is
+ * left where the forward left it */
+static int adjoint_reverse(wtd_ctx *c, int nparam, double *grad_h)
+{
+    constexpr int N = WTD_NUMEL, NH = WTD_NHIST;
+    const int S = c->S;
+    const size_t NS = (size_t)2 * S * N;
+    constexpr size_t sm = 2 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>) +
+                          80 * sizeof(double);
+    AdjWork *w = (AdjWork *)c->adj;
+    if (!w || !w->ready || w->mark_launches != c->launches || w->mark_mut != c->mut) return WTD_ERR_STATE;
+    w->ready = false;
+    const int K = w->K, nsteps = w->nsteps, nseg = w->nseg;
+    std::vector<int> &itk = w->itk;
+    double *vbar = w->fields;
+    double2 *nubar = (double2 *)(w->fields + 2 * (size_t)N);
+    WTD_CU(cudaEventRecord(w->ev[2], c->st));
 
     /* reverse sweep */
     if (nseg > 1) WTD_TRY(ck_copy(c, true, w->fin));
@@ -1937,10 +1989,29 @@ static int adjoint_run(wtd_ctx *c, int it0, int nsteps, int Kin, const double *m
     }
     if (nseg > 1) WTD_TRY(ck_copy(c, false, w->fin));
     WTD_CU(cudaMemcpyAsync(grad_h, w->dgrad, nparam * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-    return wtd_cuerr(cudaStreamSynchronize(c->st));
+    WTD_CU(cudaEventRecord(w->ev[3], c->st));
+    WTD_TRY(wtd_cuerr(cudaStreamSynchronize(c->st)));
+    w->timed_r = true;
+    /* the context is again what the forward left (the final checkpoint was restored) */
+    w->mark_launches = c->launches;
+    w->mark_mut = c->mut;
+    return WTD_OK;
+}
+
+static int adj_times(wtd_ctx *c, double *ms_forward, double *ms_reverse)
+{
+    AdjWork *w = (AdjWork *)c->adj;
+    if (!w || !w->timed_f) return WTD_ERR_STATE;
+    float a = 0.f, b = 0.f;
+    WTD_CU(cudaEventElapsedTime(&a, w->ev[0], w->ev[1]));
+    if (w->timed_r) WTD_CU(cudaEventElapsedTime(&b, w->ev[2], w->ev[3]));
+    *ms_forward = a;
+    *ms_reverse = b;
+    return WTD_OK;
 }
 #else
 static void adj_release(wtd_ctx *c) { (void)c; }
+static int adj_times(wtd_ctx *, double *, double *) { return WTD_ERR_UNSUPPORTED; }
 #endif
 
 extern "C" int wtd_adjoint(wtd_ctx *c, int it0, int nsteps, int checkpoint_every, const double *mask, int nparam,
@@ -1952,13 +2023,50 @@ extern "C" int wtd_adjoint(wtd_ctx *c, int it0, int nsteps, int checkpoint_every
 #if defined(WTD_ADJOINT_CONTACT_BDG) && defined(FAST_CONST_EFFECTIVE_MASS_MODE) && !defined(SPINSYMMETRY_MODE)
     if (c->prec != WTD_FP64 || c->staged || c->sstride != 12 * WTD_NUMEL) return WTD_ERR_UNSUPPORTED;
     WTD_CU(cudaSetDevice(c->dev));
-    const int r = adjoint_run(c, it0, nsteps, checkpoint_every, mask, nparam, loss, grad);
+    int r = adjoint_forward(c, it0, nsteps, checkpoint_every, mask, grad != NULL, loss);
+    if (r == WTD_OK && grad) r = adjoint_reverse(c, nparam, grad);
     if (r != WTD_OK) cudaStreamSynchronize(c->st);
     return r;
 #else
     (void)it0; (void)mask; (void)grad;
     return WTD_ERR_UNSUPPORTED;
 #endif
+}
+
+extern "C" int wtd_adjoint_forward(wtd_ctx *c, int it0, int nsteps, int checkpoint_every, const double *mask,
+                                   double *loss)
+{
+    if (!c || !loss || nsteps < 1 || checkpoint_every < 0) return WTD_ERR_ARG;
+#if defined(WTD_ADJOINT_CONTACT_BDG) && defined(FAST_CONST_EFFECTIVE_MASS_MODE) && !defined(SPINSYMMETRY_MODE)
+    if (c->prec != WTD_FP64 || c->staged || c->sstride != 12 * WTD_NUMEL) return WTD_ERR_UNSUPPORTED;
+    WTD_CU(cudaSetDevice(c->dev));
+    const int r = adjoint_forward(c, it0, nsteps, checkpoint_every, mask, true, loss);
+    if (r != WTD_OK) cudaStreamSynchronize(c->st);
+    return r;
+#else
+    (void)it0; (void)mask;
+    return WTD_ERR_UNSUPPORTED;
+#endif
+}
+
+extern "C" int wtd_adjoint_backward(wtd_ctx *c, int nparam, double *grad)
+{
+    if (!c || !grad || nparam < 1 || nparam > MAX_USER_PARAMS) return WTD_ERR_ARG;
+#if defined(WTD_ADJOINT_CONTACT_BDG) && defined(FAST_CONST_EFFECTIVE_MASS_MODE) && !defined(SPINSYMMETRY_MODE)
+    WTD_CU(cudaSetDevice(c->dev));
+    const int r = adjoint_reverse(c, nparam, grad);
+    if (r != WTD_OK) cudaStreamSynchronize(c->st);
+    return r;
+#else
+    return WTD_ERR_UNSUPPORTED;
+#endif
+}
+
+extern "C" int wtd_adjoint_times(wtd_ctx *c, double *ms_forward, double *ms_reverse)
+{
+    if (!c || !ms_forward || !ms_reverse) return WTD_ERR_ARG;
+    WTD_CU(cudaSetDevice(c->dev));
+    return adj_times(c, ms_forward, ms_reverse);
 }
 
 extern "C" int wtd_adjoint_release(wtd_ctx *c)

@@ -660,6 +660,41 @@ static int calculate_densities_noalloc_impl(int n, wtd_z *wf, wtd_z *dx, wtd_z *
  * -------------------------------------------------------------------------------------*/
 extern "C" {
 
+/* host forms of the energy-density-functional pieces (pca_kernels.h:11-30 and the 2D/1D
+ * headers; pca_edf.h:46-350): the uniform-solution start of the drivers (pca_uniform.h) calls
+ * them on the host.  Same published formulas as the device functional (edf:: above). */
+double polarization_h(double n_a, double n_b) { return edf::pol(n_a, n_b); }
+double der_polarization__der_na_h(double n_a, double n_b) { return edf::dpol(n_a, n_b, true); }
+double der_polarization__der_nb_h(double n_a, double n_b) { return edf::dpol(n_a, n_b, false); }
+double alpha_h(double p) { return edf::alpha(p); }
+double alpha_a_h(double p) { return edf::alpha(p); }
+double alpha_b_h(double p) { return edf::alpha(-p); }
+double alpha_plus_h(double p) { return edf::alpha_plus(p); }
+double alpha_minus_h(double p) { return edf::alpha_minus(p); }
+double der_alpha_plus__der_na_h(double n_a, double n_b)
+{
+    return edf::dap_core(edf::pol(n_a, n_b)) * edf::dpol(n_a, n_b, true);
+}
+double der_alpha_plus__der_nb_h(double n_a, double n_b)
+{
+    return edf::dap_core(edf::pol(n_a, n_b)) * edf::dpol(n_a, n_b, false);
+}
+double der_alpha_minus__der_na_h(double n_a, double n_b)
+{
+    return edf::dam_core(edf::pol(n_a, n_b)) * edf::dpol(n_a, n_b, true);
+}
+double der_alpha_minus__der_nb_h(double n_a, double n_b)
+{
+    return edf::dam_core(edf::pol(n_a, n_b)) * edf::dpol(n_a, n_b, false);
+}
+double funG_h(double p) { return edf::funG(p); }
+double funD_h(double n_a, double n_b) { return edf::funD(n_a, n_b); }
+double der_funD__der_na_h(double n_a, double n_b) { return edf::dD(n_a, n_b, true); }
+double der_funD__der_nb_h(double n_a, double n_b) { return edf::dD(n_a, n_b, false); }
+double tildeC_h(double n_a, double n_b) { return edf::tildeC(n_a, n_b); }
+double der_tildeC__der_na_h(double n_a, double n_b) { return edf::dtildeC(n_a, n_b, true); }
+double der_tildeC__der_nb_h(double n_a, double n_b) { return edf::dtildeC(n_a, n_b, false); }
+
 int memcopy_const(double mu_a, double mu_b, double ec, double t0, double dt, double kF)
 {
     double eF = kF * kF / 2., nF = kF * kF * kF / (3. * M_PI * M_PI);

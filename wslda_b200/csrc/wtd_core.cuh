@@ -330,6 +330,14 @@ __device__ __forceinline__ void st_keep(double *a, double v, uint64_t pol)
 {
     asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
 }
+/* *a += v as a reduction performed in L2 (no value returned, so the thread does not wait for
+ * it), with the same policy.  Used where every address of a slot is updated by one thread
+ * only: reductions of one thread to one address take effect in program order, so the sum's
+ * order, and therefore its rounding, is that of a plain read-modify-write loop. */
+__device__ __forceinline__ void red_keep(double *a, double v, uint64_t pol)
+{
+    asm volatile("red.relaxed.gpu.global.add.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
 
 /* streaming loads/stores (evict-first): state and history arrays are touched once per pass */
 __device__ __forceinline__ double2 ld_stream(const double2 *p) { return __ldcs(p); }

@@ -47,13 +47,13 @@ __device__ __forceinline__ void wtd_decode(int i, int &ix, int &iy, int &iz)
 
 namespace edf {
 /* pca_edf.h:17-33 */
-__device__ __forceinline__ double p_reg(double n)
+__host__ __device__ __forceinline__ double p_reg(double n)
 {
     if (n <= P_NMIN) return 0.0;
     if (n >= P_NMAX) return 1.0;
     return 0.5 + 0.5 * tanh(P_ALPHA * tan((M_PI * (n - P_NMIN)) / (P_NMAX - P_NMIN) - M_PI / 2.0));
 }
-__device__ __forceinline__ double dp_reg(double n)
+__host__ __device__ __forceinline__ double dp_reg(double n)
 {
     if (n <= P_NMIN || n >= P_NMAX) return 0.0;
     double a = (M_PI * (n - P_NMIN)) / (P_NMAX - P_NMIN) - M_PI / 2.0;
@@ -61,12 +61,12 @@ __device__ __forceinline__ double dp_reg(double n)
     return 0.5 * P_ALPHA * M_PI / (c * c) / (P_NMAX - P_NMIN);
 }
 /* pca_edf.h:39-97 */
-__device__ __forceinline__ double pol(double a, double b)
+__host__ __device__ __forceinline__ double pol(double a, double b)
 {
     double pr = p_reg(a + b);
     return pr == 0.0 ? 0.0 : pr * (a - b) / (a + b);
 }
-__device__ __forceinline__ double dpol(double a, double b, bool wrt_a)
+__host__ __device__ __forceinline__ double dpol(double a, double b, bool wrt_a)
 {
     double np = a + b, pr = p_reg(np), dpr = dp_reg(np), r = 0.0;
     if (pr != 0.0) r += pr * (wrt_a ? 2.0 * b : -2.0 * a) / (np * np);
@@ -74,32 +74,32 @@ __device__ __forceinline__ double dpol(double a, double b, bool wrt_a)
     return r;
 }
 /* pca_edf.h:102-211 */
-__device__ __forceinline__ double alpha(double p)
+__host__ __device__ __forceinline__ double alpha(double p)
 {
     double p2 = p * p, p4 = p2 * p2;
     return A0 + A1 * p * (1.0 - (2.0 / 3.0) * p2 + (1.0 / 5.0) * p4) + A2 * p2 * (1.0 - p2 + (1.0 / 3.0) * p4);
 }
-__device__ __forceinline__ double alpha_plus(double p) { return 0.5 * (alpha(p) + alpha(-p)); }
-__device__ __forceinline__ double alpha_minus(double p) { return 0.5 * (alpha(p) - alpha(-p)); }
-__device__ __forceinline__ double dap_core(double p)
+__host__ __device__ __forceinline__ double alpha_plus(double p) { return 0.5 * (alpha(p) + alpha(-p)); }
+__host__ __device__ __forceinline__ double alpha_minus(double p) { return 0.5 * (alpha(p) - alpha(-p)); }
+__host__ __device__ __forceinline__ double dap_core(double p)
 {
     double p2 = p * p, p4 = p2 * p2;
     return 2.0 * A2 * p * (1.0 - p2 + (1.0 / 3.0) * p4) - 2.0 * A2 * p * p2 * (1.0 - (2.0 / 3.0) * p2);
 }
-__device__ __forceinline__ double dam_core(double p)
+__host__ __device__ __forceinline__ double dam_core(double p)
 {
     double p2 = p * p, p4 = p2 * p2;
     return A1 * (1.0 - (2.0 / 3.0) * p2 + (1.0 / 5.0) * p4) - 4.0 * A1 * p2 * ((1.0 / 3.0) - (1.0 / 5.0) * p2);
 }
 /* pca_edf.h:216-311 */
-__device__ __forceinline__ double funG(double p) { return G0 + G1 * p * p; }
-__device__ __forceinline__ double funD(double a, double b)
+__host__ __device__ __forceinline__ double funG(double p) { return G0 + G1 * p * p; }
+__host__ __device__ __forceinline__ double funD(double a, double b)
 {
     double p = pol(a, b);
     return (1.0 / (20.0 * M_PI * M_PI)) * pow(6.0 * M_PI * M_PI * (a + b), 5.0 / 3.0) *
            (funG(p) - alpha(p) * pow((1.0 + p) / 2.0, 5.0 / 3.0) - alpha(-p) * pow((1.0 - p) / 2.0, 5.0 / 3.0));
 }
-__device__ __forceinline__ double dD(double a, double b, bool wrt_a)
+__host__ __device__ __forceinline__ double dD(double a, double b, bool wrt_a)
 {
     double p = pol(a, b);
     double dA = dam_core(p), dB = dap_core(p);
@@ -112,11 +112,11 @@ __device__ __forceinline__ double dD(double a, double b, bool wrt_a)
     return t1 + t2;
 }
 /* pca_edf.h:316-350 */
-__device__ __forceinline__ double tildeC(double a, double b)
+__host__ __device__ __forceinline__ double tildeC(double a, double b)
 {
     return alpha_plus(pol(a, b)) * pow(a + b + DENSEPSILON, 1.0 / 3.0) / GAMMA0;
 }
-__device__ __forceinline__ double dtildeC(double a, double b, bool wrt_a)
+__host__ __device__ __forceinline__ double dtildeC(double a, double b, bool wrt_a)
 {
     return (dap_core(pol(a, b)) * dpol(a, b, wrt_a) * pow(a + b + DENSEPSILON, 1.0 / 3.0) +
             (1.0 / 3.0) * alpha_plus(pol(a, b)) * pow(a + b + DENSEPSILON, -2.0 / 3.0)) / GAMMA0;

@@ -96,10 +96,16 @@ __device__ __forceinline__ void plane_h_axis(const typename cplx<TC>::t *P, type
         team_fwd<n, T>(v, scr, g, tw);
         team_mul_lap<n, T>(v, lapk, g);
         team_inv<n, T>(v, scr, g, tw);
+        /* the plane's K values of the line are read before any is written (here and below), so
+         * that the shared-memory round trips overlap */
+        C hk[n1];
 #pragma unroll
         for (int i = 0; i < n1; i++) {
-            C h;
-            if (first) { h.x = (TC)0; h.y = (TC)0; } else h = Kp[at(i)];
+            if (first) { hk[i].x = (TC)0; hk[i].y = (TC)0; } else hk[i] = Kp[at(i)];
+        }
+#pragma unroll
+        for (int i = 0; i < n1; i++) {
+            C h = hk[i];
             h.x += sgn * (TC)-0.25 * v[i].x; h.y += sgn * (TC)-0.25 * v[i].y;
             Kp[at(i)] = h;
         }
@@ -113,10 +119,13 @@ __device__ __forceinline__ void plane_h_axis(const typename cplx<TC>::t *P, type
         const int Ac = (comp ? CF_ABX : CF_AAX) + ax;
         team_mul_d<n, T>(w, dk, g);
         team_inv<n, T>(w, scr, g, tw);
+        C hk[n1];
+#pragma unroll
+        for (int i = 0; i < n1; i++) hk[i] = Kp[at(i)];
 #pragma unroll
         for (int i = 0; i < n1; i++) {
             const TC A = (TC)CFP(Ac, pt(i));
-            C h = Kp[at(i)];
+            C h = hk[i];
             h.x += A * w[i].y; h.y += -A * w[i].x;
             Kp[at(i)] = h;
         }
@@ -124,11 +133,15 @@ __device__ __forceinline__ void plane_h_axis(const typename cplx<TC>::t *P, type
     team_mul_lap<n, T>(v, lapk, g);
     team_inv<n, T>(v, scr, g, tw);
     const int aco = comp ? CF_AB : CF_AA;
+    C hk[n1];
+#pragma unroll
+    for (int i = 0; i < n1; i++) {
+        if (first && !VAR) { hk[i].x = (TC)0; hk[i].y = (TC)0; } else hk[i] = Kp[at(i)];
+    }
 #pragma unroll
     for (int i = 0; i < n1; i++) {
         const TC a = sgn * (TC)CFP(aco, pt(i));
-        C h;
-        if (first && !VAR) { h.x = (TC)0; h.y = (TC)0; } else h = Kp[at(i)];
+        C h = hk[i];
         h.x += a * v[i].x; h.y += a * v[i].y;
         Kp[at(i)] = h;
     }
@@ -208,23 +221,56 @@ template <typename TC, int CL, int TX_, int HPAD> struct XSmem {
     static constexpr size_t hs = (size_t)LINES * HP * sizeof(C);            /* H, then the update, per line */
     static constexpr size_t scr = (size_t)LINES * team_scratch(NX, TX) * sizeof(C);
     static constexpr size_t red = 80 * sizeof(double);
-    static constexpr size_t bytes = tab + hs + scr + red;
+    static constexpr size_t base = tab + hs + scr + red;
+    /* FP64 slabs of the local-term coefficients at this CTA's columns, loaded once per launch
+     * (the coefficients are the same for every state): DRE, DIM, V_a, V_b and, with variable
+     * mass, N_a, N_b, CJ_a, CJ_b — as many of these as fit beside the rest (8, 4 or none);
+     * rows of CP doubles, padded so that the 16 lanes of a half warp (4 x-rows of 4 columns)
+     * fall on distinct banks */
+    static constexpr int CP = QC + 4;
+    static constexpr size_t slab = (size_t)NX * CP * sizeof(double);
+    static constexpr int NCW = WTD_VAR ? 8 : 4;
+    static constexpr int NCS = base + (size_t)NCW * slab + 64 <= WTD_SMEM_MAX ? NCW
+                             : base + 4 * slab + 64 <= WTD_SMEM_MAX ? 4 : 0;
+    static constexpr size_t bytes = base + (size_t)NCS * slab;
     static constexpr bool ok = WTD_L_NYZ % CL == 0 && XT <= 1024 && XT % 32 == 0 && NX % (TX * TX) == 0;
 };
 
-/* sum over the cluster of one double per CTA, in rank order (the same result on every CTA).
- * Consecutive calls alternate between two slots: the value a CTA writes in call k goes where
- * call k-2 put its value, and every CTA finished reading call k-2 before it arrived at the
- * barrier of call k-1, so no value is overwritten while another CTA may still read it. */
+/* the CF_* list entry of coefficient slab k */
+__device__ __forceinline__ int xslab_cf(int k)
+{
+    return k == 0 ? CF_DRE : k == 1 ? CF_DIM : k < 4 ? CF_VA + (k - 2) : k < 6 ? CF_NA + (k - 4) : CF_CJA + (k - 6);
+}
+
+/* Sum over the cluster of one double per thread, in two halves.  cluster_post adds the CTA's
+ * values (warp sums, then warp 0 over the warp sums — the order of block_sum), publishes the
+ * CTA's partial in its slot and arrives on the cluster barrier without waiting; cluster_collect
+ * waits and adds the CTA partials in rank order (the same result on every CTA).  Work placed
+ * between the two overlaps the barrier.  Consecutive sums alternate between two slots: the
+ * partial of sum k goes where sum k-2 put its own, which every CTA finished reading before it
+ * arrived for sum k-1, and it is only written after the wait of sum k-1 — so no partial is
+ * overwritten while another CTA may still read it.  The warp-sum array red is rewritten only
+ * after the wait of the previous sum, by which time warp 0 has read it. */
 template <int CL>
-__device__ __forceinline__ double cluster_sum(double v, double *cred, int &calls)
+__device__ __forceinline__ void cluster_post(double v, double *red, double *cred, int slot)
+{
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        double s = (lane < nw) ? red[lane] : 0.0;
+        s = warp_sum(s);
+        if (lane == 0) cred[slot] = s;
+    }
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+template <int CL>
+__device__ __forceinline__ double cluster_collect(double *cred, int slot)
 {
     namespace cg = cooperative_groups;
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
     cg::cluster_group cl = cg::this_cluster();
-    const int slot = calls & 1;
-    calls++;
-    if (threadIdx.x == 0) cred[slot] = v;
-    cl.sync();
     double s = 0.0;
 #pragma unroll
     for (int r = 0; r < CL; r++) s += *cl.map_shared_rank(cred + slot, r);
@@ -245,6 +291,8 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
     C *Hs = (C *)(smem_raw + SM::tab);                 /* [line][HP] */
     C *Scr = Hs + SM::LINES * HP;                      /* [line][team scratch] */
     double *red = (double *)(smem_raw + SM::tab + SM::hs + SM::scr);
+    double *cs = (double *)(smem_raw + SM::base);        /* [NCS][NX][CP] coefficient slabs */
+    constexpr int NCS = SM::NCS, CP = SM::CP, SL = NX * CP;
     __shared__ double cred[2];
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
@@ -269,6 +317,13 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
         ds[2 * (size_t)p + 1] = 0.0;
 #pragma unroll
         for (int w = 2; w < 12; w++) ds[(size_t)w * N + p] = 0.0;
+    }
+    for (int k = 0; k < NCS; k++) {
+        const double *src = a.cf + (size_t)xslab_cf(k) * N + rank * QC;
+        for (int i = t; i < NX * QC; i += XT) {
+            const int x = i / QC, jj = i - x * QC;
+            cs[k * SL + x * CP + jj] = src[(size_t)x * NYZ + jj];
+        }
     }
     __syncthreads();
     int ncalls = 0;   /* cluster sums so far (slot alternation) */
@@ -306,32 +361,35 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
         const size_t ub = (size_t)n * N, vb = SN + (size_t)n * N;
         const bool haveH = (PASS == 1) || (PASS == 3) || (PASS == 0 && !a.fk_given);
         double E = 0.0;
+        int eslot = 0;
         if (haveH) {
             /* K_yz plus the local terms (pca_kernels.cu:233-391) at this thread's points */
 #pragma unroll 2
             for (int i = 0; i < n1; i++) {
                 const int x = g + TX * i, p = x * NYZ + q;
                 const double2 u = to_d(Y[ub + p]), v = to_d(Y[vb + p]);
-                const double va = ld_ro_keep(cf + CF_VA * (size_t)N + p, pol), vbb = ld_ro_keep(cf + CF_VB * (size_t)N + p, pol);
-                const double dr = ld_ro_keep(cf + CF_DRE * (size_t)N + p, pol), di = ld_ro_keep(cf + CF_DIM * (size_t)N + p, pol);
+                /* this component's coefficients: from the slabs, else from L2 */
+                auto co = [&](int k) -> double {
+                    return k < NCS ? cs[k * SL + x * CP + j] : ld_ro_keep(cf + (size_t)xslab_cf(k) * N + p, pol);
+                };
+                const double vs = co(2 + comp), dr = co(0), di = co(1);
                 double2 h;
                 if (VAR) {
-                    const double na = ld_ro_keep(cf + CF_NA * (size_t)N + p, pol), nb = ld_ro_keep(cf + CF_NB * (size_t)N + p, pol);
-                    const double cja = ld_ro_keep(cf + CF_CJA * (size_t)N + p, pol), cjb = ld_ro_keep(cf + CF_CJB * (size_t)N + p, pol);
+                    const double ns = co(4 + comp), cj = co(6 + comp);
                     if (comp == 0) {
-                        h.x = va * u.x - cja * u.y + (dr * v.x - di * v.y) + na * u.x;
-                        h.y = va * u.y + cja * u.x + (dr * v.y + di * v.x) + na * u.y;
+                        h.x = vs * u.x - cj * u.y + (dr * v.x - di * v.y) + ns * u.x;
+                        h.y = vs * u.y + cj * u.x + (dr * v.y + di * v.x) + ns * u.y;
                     } else {
-                        h.x = -(vbb * v.x + cjb * v.y) + (dr * u.x + di * u.y) - nb * v.x;
-                        h.y = -(vbb * v.y - cjb * v.x) + (dr * u.y - di * u.x) - nb * v.y;
+                        h.x = -(vs * v.x + cj * v.y) + (dr * u.x + di * u.y) - ns * v.x;
+                        h.y = -(vs * v.y - cj * v.x) + (dr * u.y - di * u.x) - ns * v.y;
                     }
                 } else {
                     if (comp == 0) {
-                        h.x = va * u.x + (dr * v.x - di * v.y);
-                        h.y = va * u.y + (dr * v.y + di * v.x);
+                        h.x = vs * u.x + (dr * v.x - di * v.y);
+                        h.y = vs * u.y + (dr * v.y + di * v.x);
                     } else {
-                        h.x = -vbb * v.x + (dr * u.x + di * u.y);
-                        h.y = -vbb * v.y + (dr * u.y - di * u.x);
+                        h.x = -vs * v.x + (dr * u.x + di * u.y);
+                        h.y = -vs * v.y + (dr * u.y - di * u.x);
                     }
                 }
                 const C k = Kin[fb + p];
@@ -392,15 +450,34 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
                 const double2 y = to_d(Y[fb + p]);
                 e += y.x * (double)h.x + y.y * (double)h.y;
             }
-            E = cluster_sum<CL>(block_sum(e, red), cred, ncalls) * WTD_DV;
+            eslot = ncalls & 1;
+            ncalls++;
+            cluster_post<CL>(e, red, cred, eslot);
+        }
+        /* the ABM inputs of this thread's points, loaded while the cluster sum of <H> completes:
+         * y and the first NRP history slots this pass reads */
+        constexpr int NR = (PASS == 0) ? NH - 1 : (PASS == 1 ? 1 : 0);
+        constexpr int NRP = (PASS == 0) ? (sizeof(TH) == 8 ? 2 : 1) : (PASS == 1 ? 1 : 0);
+        auto ring = [&](int k) -> const TH * { return (const TH *)xa.s.slot[PASS == 1 ? NH - 2 : k]; };
+        TY y0r[n1];
+        TH frr[NRP > 0 ? NRP : 1][n1];
+#pragma unroll
+        for (int i = 0; i < n1; i++) {
+            const size_t gi = fb + (size_t)(g + TX * i) * NYZ + q;
+            y0r[i] = Y[gi];
+#pragma unroll
+            for (int k = 0; k < NRP; k++) frr[k][i] = ld_stream(ring(k) + gi);
+        }
+        if (haveH) {
+            E = cluster_collect<CL>(cred, eslot) * WTD_DV;
             if (t == 0 && rank == 0) a.qpe[n] = E;
         }
         if (PASS == 3) {
-#pragma unroll 2
+#pragma unroll
             for (int i = 0; i < n1; i++) {
                 const int x = g + TX * i;
                 const size_t gi = fb + x * NYZ + q;
-                const double2 y0 = to_d(Y[gi]);
+                const double2 y0 = to_d(y0r[i]);
                 const C h = Hl[x];
                 ((TH *)xa.s.slot[NH - 1])[gi] = from_d<TH>(make_double2((double)h.x - E * y0.x, (double)h.y - E * y0.y));
             }
@@ -409,20 +486,15 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
         }
         /* ---- ABM update of this thread's points, unnormalised into H ---- */
         double nrm = 0.0;
-        constexpr int NR = (PASS == 0) ? NH - 1 : (PASS == 1 ? 1 : 0);
-#pragma unroll 2
+#pragma unroll
         for (int i = 0; i < n1; i++) {
             const int x = g + TX * i;
             const size_t gi = fb + x * NYZ + q;
-            const double2 y0 = to_d(Y[gi]);
+            const double2 y0 = to_d(y0r[i]);
             double2 fr[NR > 0 ? NR : 1], fkg = make_double2(0.0, 0.0);
-            if (PASS == 0) {
 #pragma unroll
-                for (int k = 0; k < NR; k++) fr[k] = to_d(ld_stream((const TH *)xa.s.slot[k] + gi));
-                if (!haveH) fkg = to_d(ld_stream((const TH *)xa.s.slot[NH - 1] + gi));
-            } else if (PASS == 1) {
-                fr[0] = to_d(ld_stream((const TH *)xa.s.slot[NH - 2] + gi));
-            }
+            for (int k = 0; k < NR; k++) fr[k] = to_d(k < NRP ? frr[k < NRP ? k : 0][i] : ld_stream(ring(k) + gi));
+            if (PASS == 0 && !haveH) fkg = to_d(ld_stream((const TH *)xa.s.slot[NH - 1] + gi));
             double2 fk = make_double2(0.0, 0.0);
             if (PASS != 2) {
                 if (haveH) {
@@ -460,7 +532,10 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
             C r; r.x = (TC)out.x; r.y = (TC)out.y;
             Hl[x] = r;
         }
-        const double nrm_tot = sqrt(cluster_sum<CL>(block_sum(nrm, red), cred, ncalls) * WTD_DV);
+        const int nslot = ncalls & 1;
+        ncalls++;
+        cluster_post<CL>(nrm, red, cred, nslot);
+        const double nrm_tot = sqrt(cluster_collect<CL>(cred, nslot) * WTD_DV);
         const double cinv = 1.0 / nrm_tot;
         if (a.nrm_out && t == 0 && rank == 0) a.nrm_out[n] = nrm_tot;
         /* ---- normalise, store; the stored values are what the densities see ---- */
@@ -481,7 +556,8 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
             const int x = i / QC, jj = i - x * QC;
             const int p = x * NYZ + rank * QC + jj;
             const C hu = Hs[jj * HP + x], hv = Hs[(QC + jj) * HP + x];
-            dens_limited(ds, p, N, make_double2((double)hu.x, (double)hu.y), make_double2((double)hv.x, (double)hv.y), f, wgt, pol);
+            dens_limited_red(ds, p, N, make_double2((double)hu.x, (double)hu.y), make_double2((double)hv.x, (double)hv.y), f, wgt,
+                             pol);
         }
         if (GRAD) {
             /* x-parts of tau_tmp = Re[psi* lap psi] and j_x = Im[psi* d_x psi] (pca_dens.cu:41-108) */
@@ -502,8 +578,8 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
             for (int i = 0; i < n1; i++) {
                 const int x = g + TX * i, p = x * NYZ + q;
                 const C s = Hl[x];
-                ds[(size_t)j_q * N + p] += jsgn * ((double)s.x * (double)w[i].y - (double)s.y * (double)w[i].x) * fw;
-                ds[(size_t)tau_q * N + p] += ((double)s.x * (double)v[i].x + (double)s.y * (double)v[i].y) * fw;
+                red_keep(ds + (size_t)j_q * N + p, jsgn * ((double)s.x * (double)w[i].y - (double)s.y * (double)w[i].x) * fw, pol);
+                red_keep(ds + (size_t)tau_q * N + p, ((double)s.x * (double)v[i].x + (double)s.y * (double)v[i].y) * fw, pol);
             }
         }
         __syncthreads();
@@ -536,11 +612,22 @@ __device__ __forceinline__ void plane_dens_axis(const typename cplx<TC>::t *P, t
     team_inv<n, T>(w, scr, g, tw);
     team_mul_lap<n, T>(v, lapk, g);
     team_inv<n, T>(v, scr, g, tw);
+    /* accumulators read before any is written (half a line at a time), so that the shared-memory
+     * round trips overlap instead of forming one chain */
+    constexpr int HB = n1 > 4 ? n1 / 2 : n1;
 #pragma unroll
-    for (int i = 0; i < n1; i++) {
-        const C s = P[at(i)];
-        aj[ai(i)] += jsgn * ((double)s.x * (double)w[i].y - (double)s.y * (double)w[i].x) * fw;
-        acc[ai(i)] += ((double)s.x * (double)v[i].x + (double)s.y * (double)v[i].y) * fw;
+    for (int i0 = 0; i0 < n1; i0 += HB) {
+        double tj[HB], ta[HB];
+#pragma unroll
+        for (int i = 0; i < HB; i++) { tj[i] = aj[ai(i0 + i)]; ta[i] = acc[ai(i0 + i)]; }
+#pragma unroll
+        for (int i = 0; i < HB; i++) {
+            const C s = P[at(i0 + i)];
+            tj[i] += jsgn * ((double)s.x * (double)w[i0 + i].y - (double)s.y * (double)w[i0 + i].x) * fw;
+            ta[i] += ((double)s.x * (double)v[i0 + i].x + (double)s.y * (double)v[i0 + i].y) * fw;
+        }
+#pragma unroll
+        for (int i = 0; i < HB; i++) { aj[ai(i0 + i)] = tj[i]; acc[ai(i0 + i)] = ta[i]; }
     }
 }
 

@@ -18,8 +18,10 @@
  *
  * HBM traffic per state and pass is the compulsory stream: pass A reads y and the q history
  * slots and writes f_k, y_pred and P; pass B reads y_pred and P and writes y_{k+1}.  The
- * density sums of the states a CTA processes accumulate in a private FP64 slot (plain
- * read-modify-write, no atomics, deterministic) that a second kernel reduces in fixed order.
+ * density sums of the states a CTA processes accumulate in a private FP64 slot that a second
+ * kernel reduces in fixed order.  Every word of a slot is updated by one thread only, as L2
+ * reductions (red.add, the thread does not wait for the old value) that take effect in program
+ * order: the sum and its rounding are those of a plain read-modify-write loop, deterministic.
  *
  * Precision forms (template arguments): TY = storage of y (double2 or float2), TH = storage
  * of history and P, TC = arithmetic of the FFT and H psi.  The ABM combination, the norms,
@@ -336,28 +338,16 @@ __device__ __forceinline__ void dens_limited(double *ds, int p, int N, double2 u
     st_keep(a3, s3 + (v.x * v.x + v.y * v.y) * fb, pol);
 }
 
-/* the same for two points at once (q valid when hq): all slot loads are issued before any
- * store, so the two points share one L2 round trip (the loads and stores carry cache hints as
- * volatile asm, which keeps them in program order) */
-__device__ __forceinline__ void dens_limited2(double *ds, int p, int q, bool hq, int N, double2 u, double2 v,
-                                              double2 u1, double2 v1, double f, double w, uint64_t pol)
+/* the same as reductions performed in L2 (red_keep): the thread does not wait for the slot's
+ * old values; every word of the slot must be updated by this one thread only */
+__device__ __forceinline__ void dens_limited_red(double *ds, int p, int N, double2 u, double2 v, double f, double w,
+                                                 uint64_t pol)
 {
     double fa = f * w, fb = (1.0 - f) * w, fn = (1.0 - 2.0 * f) * 0.5 * w;
-    double *a0 = ds + 2 * p, *a1 = ds + 2 * p + 1, *a2 = ds + 2 * (size_t)N + p, *a3 = ds + 7 * (size_t)N + p;
-    double *b0 = ds + 2 * q, *b1 = ds + 2 * q + 1, *b2 = ds + 2 * (size_t)N + q, *b3 = ds + 7 * (size_t)N + q;
-    double s0 = ld_keep(a0, pol), s1 = ld_keep(a1, pol), s2 = ld_keep(a2, pol), s3 = ld_keep(a3, pol);
-    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
-    if (hq) { t0 = ld_keep(b0, pol); t1 = ld_keep(b1, pol); t2 = ld_keep(b2, pol); t3 = ld_keep(b3, pol); }
-    st_keep(a0, s0 + (u.x * v.x + u.y * v.y) * fn, pol);
-    st_keep(a1, s1 + (u.y * v.x - u.x * v.y) * fn, pol);
-    st_keep(a2, s2 + (u.x * u.x + u.y * u.y) * fa, pol);
-    st_keep(a3, s3 + (v.x * v.x + v.y * v.y) * fb, pol);
-    if (hq) {
-        st_keep(b0, t0 + (u1.x * v1.x + u1.y * v1.y) * fn, pol);
-        st_keep(b1, t1 + (u1.y * v1.x - u1.x * v1.y) * fn, pol);
-        st_keep(b2, t2 + (u1.x * u1.x + u1.y * u1.y) * fa, pol);
-        st_keep(b3, t3 + (v1.x * v1.x + v1.y * v1.y) * fb, pol);
-    }
+    red_keep(ds + 2 * p, (u.x * v.x + u.y * v.y) * fn, pol);
+    red_keep(ds + 2 * p + 1, (u.y * v.x - u.x * v.y) * fn, pol);
+    red_keep(ds + 2 * (size_t)N + p, (u.x * u.x + u.y * u.y) * fa, pol);
+    red_keep(ds + 7 * (size_t)N + p, (v.x * v.x + v.y * v.y) * fb, pol);
 }
 
 /* tau and j contributions of one normalised component (pca_dens.cu:41-108).  B0 holds the
@@ -379,6 +369,8 @@ __device__ __forceinline__ void dens_gradients(double *ds, const TY *ysrc, typen
     const double fq = (1.0 - 2.0 * f) * w * -0.5;
     const int tau_q = comp == 0 ? 3 : 8, j_q = comp == 0 ? 4 : 9;
     const double jsgn = comp == 0 ? 1.0 : -1.0;
+    /* slot updates as L2 reductions: each word of the CTA's slot is updated by one thread only */
+    const uint64_t pol = l2_policy_keep();
     __syncthreads();
     fft_forward<G, 1>(B0, 0, tw);
     for (int op = 0; op <= G::dims; op++) {
@@ -396,24 +388,24 @@ __device__ __forceinline__ void dens_gradients(double *ds, const TY *ysrc, typen
             double dx = d.x, dy = d.y;
             if (op == 0) {
                 double lx = dx - sv.x * kp2, ly = dy - sv.y * kp2;
-                ds[tau_q * (size_t)N + p] += (sv.x * lx + sv.y * ly) * fw;
+                red_keep(ds + tau_q * (size_t)N + p, (sv.x * lx + sv.y * ly) * fw, pol);
                 if (yother) {
                     const double2 o = to_d(yother[p]);
                     const double im = sv.x * ly - sv.y * lx; /* Im[psi* lap psi] */
                     if (comp == 0) {
-                        ds[12 * (size_t)N + p] += im * fw;
+                        red_keep(ds + 12 * (size_t)N + p, im * fw, pol);
                         /* v* lap u */
-                        ds[14 * (size_t)N + 2 * p] += (o.x * lx + o.y * ly) * fq;
-                        ds[14 * (size_t)N + 2 * p + 1] += (o.x * ly - o.y * lx) * fq;
+                        red_keep(ds + 14 * (size_t)N + 2 * p, (o.x * lx + o.y * ly) * fq, pol);
+                        red_keep(ds + 14 * (size_t)N + 2 * p + 1, (o.x * ly - o.y * lx) * fq, pol);
                     } else {
-                        ds[13 * (size_t)N + p] -= im * fw;
+                        red_keep(ds + 13 * (size_t)N + p, -(im * fw), pol);
                         /* (lap v)* u */
-                        ds[14 * (size_t)N + 2 * p] += (lx * o.x + ly * o.y) * fq;
-                        ds[14 * (size_t)N + 2 * p + 1] += (lx * o.y - ly * o.x) * fq;
+                        red_keep(ds + 14 * (size_t)N + 2 * p, (lx * o.x + ly * o.y) * fq, pol);
+                        red_keep(ds + 14 * (size_t)N + 2 * p + 1, (lx * o.y - ly * o.x) * fq, pol);
                     }
                 }
             } else {
-                ds[(j_q + op - 1) * (size_t)N + p] += jsgn * (sv.x * dy - sv.y * dx) * fw;
+                red_keep(ds + (j_q + op - 1) * (size_t)N + p, jsgn * (sv.x * dy - sv.y * dx) * fw, pol);
             }
         }
         __syncthreads();
@@ -605,7 +597,8 @@ wtd_fused_pass(StepArgs a, const double2 *gtw, const double *gk)
                     HU[o] = cu; HV[o] = cv;
                 }
             }
-            dens_limited2(ds, p, q, hq, N, uu[0], vv[0], uu[1], vv[1], f, w, pol);
+            dens_limited_red(ds, p, N, uu[0], vv[0], f, w, pol);
+            if (hq) dens_limited_red(ds, q, N, uu[1], vv[1], f, w, pol);
         }
         if (GRAD) {
             /* const mass: (HU, HV) = (BU, BV) hold the state, B2 is work.
