@@ -577,7 +577,7 @@ def probe(args):
     measurement and --warmup steps (the case the ncu captures of the line path run)"""
     import torch
     from wslda_b200 import TDRun
-    wl = WORKLOADS[args.workload]
+    wl = C5 if args.workload == "c5" else WORKLOADS[args.workload]
     nwf = args.nwf or wl["nwf"]
     proj, d = make_inputs(wl["project"], nwf)
     r = TDRun(wl["project"], nwf, precision=args.probe, device=0)
@@ -609,7 +609,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--blocks", type=int, default=3, help="timed blocks of --steps steps each; value is the median block")
     ap.add_argument("--impl", default="wtd", choices=["wtd", "reference"])
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c5"],
+                    help="c5 (reported inside the default run's line) only with --probe")
     ap.add_argument("--fp64-only", action="store_true")
     ap.add_argument("--nwf", type=int, default=0, help="override the workload's state count (small profiling cases)")
     ap.add_argument("--no-cpu", action="store_true")
@@ -638,7 +639,7 @@ def main():
     args.blocks = max(args.blocks, 1)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    wl = WORKLOADS[args.workload]
+    wl = WORKLOADS.get(args.workload, C5)
     metric = "qp-state*steps/s"
     cfg = {"workload": wl["desc"], "project": wl["project"], "states": args.nwf or wl["nwf"], "precision": "fp64",
            "l2": "inputs larger than L2 (state arrays of GBs)", "parallelism": f"states sharded over {world} GPU(s)"}
@@ -670,6 +671,8 @@ def main():
     if args.probe >= 0:
         print(json.dumps(probe(args)))
         return
+    if args.workload == "c5":
+        ap.error("--workload c5 needs --probe")
 
     if world > 1:
         import torch

@@ -176,8 +176,9 @@ int wtd_adjoint_release(wtd_ctx *ctx);
  * wtd_adjoint_forward runs the forward of wtd_adjoint with its checkpoints and records and
  * returns L; wtd_adjoint_backward then runs the reverse sweep and returns dL/dparams[0..nparam).
  * Between the two the context must not change: any launch, upload or setter on it makes the
- * backward return WTD_ERR_STATE (so does a backward without a forward).  After the backward the
- * context is again where the forward left it, and a second backward may follow. */
+ * backward return WTD_ERR_STATE (so does a backward without a forward, or a second backward:
+ * the reverse sweep reuses the forward's records).  After the backward the context is again
+ * where the forward left it. */
 int wtd_adjoint_forward(wtd_ctx *ctx, int it0, int nsteps, int checkpoint_every, const double *mask, double *loss);
 int wtd_adjoint_backward(wtd_ctx *ctx, int nparam, double *grad);
 /* device time of the last adjoint forward (initial measurement, nsteps steps with checkpoints

@@ -616,7 +616,7 @@ static int line_launch_h(wtd_ctx *c, const void *y)
     typedef PlaneSmem<TC> SM;
     auto k = k3_plane_h<TY, TC, WTD_VAR>;
     WTD_ONCE_PER_DEVICE(WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::h_bytes)));
-    k<<<c->p1grid, PlaneGeo::PT, SM::h_bytes, c->st>>>((const TY *)y, (typename cplx<TC>::t *)c->kbuf, c->cf, c->S, c->tw,
+    k<<<c->p1grid, PlaneGeo::PT * SM::HS, SM::h_bytes, c->st>>>((const TY *)y, (typename cplx<TC>::t *)c->kbuf, c->cf, c->S, c->tw,
                                                         c->ktab);
     WTD_LAUNCHED(c);
     return WTD_OK;
@@ -721,8 +721,10 @@ static int line_setup_t(wtd_ctx *c, int nsm)
         typedef PlaneSmem<TC> SM;
         auto k = k3_plane_h<TY, TC, WTD_VAR>;
         WTD_CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::h_bytes));
-        WTD_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, PlaneGeo::PT, SM::h_bytes));
-        c->p1grid = nsm * (per > 0 ? per : 1);
+        WTD_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, PlaneGeo::PT * SM::HS, SM::h_bytes));
+        /* a whole number of CTAs per (component, x-plane) pair */
+        const int pairs = 2 * NX, nch = nsm * (per > 0 ? per : 1) / pairs;
+        c->p1grid = pairs * (nch > 0 ? nch : 1);
         auto kd = k3_plane_dens<TY, TC>;
         WTD_CU(cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::d_bytes));
         WTD_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kd, PlaneGeo::PT, SM::d_bytes));
@@ -1848,7 +1850,8 @@ static int adj_choose_K(wtd_ctx *c, int nsteps, int K)
 static int adjoint_forward(wtd_ctx *c, int it0, int nsteps, int Kin, const double *mask_h, bool record, double *loss_h)
 {
     constexpr int N = WTD_NUMEL;
-    constexpr size_t sm = 2 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>) +
+    /* the reverse kernels' shared memory: two pairs of field buffers, tables, block-sum words */
+    constexpr size_t sm = 4 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>) +
                           80 * sizeof(double);
     if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     const int K = record ? adj_choose_K(c, nsteps, Kin) : 0;
@@ -1898,7 +1901,8 @@ static int adjoint_reverse(wtd_ctx *c, int nparam, double *grad_h)
     constexpr int N = WTD_NUMEL, NH = WTD_NHIST;
     const int S = c->S;
     const size_t NS = (size_t)2 * S * N;
-    constexpr size_t sm = 2 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>) +
+    /* the reverse kernels' shared memory: two pairs of field buffers, tables, block-sum words */
+    constexpr size_t sm = 4 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>) +
                           80 * sizeof(double);
     AdjWork *w = (AdjWork *)c->adj;
     if (!w || !w->ready || w->mark_launches != c->launches || w->mark_mut != c->mut) return WTD_ERR_STATE;
@@ -1992,9 +1996,6 @@ static int adjoint_reverse(wtd_ctx *c, int nparam, double *grad_h)
     WTD_CU(cudaEventRecord(w->ev[3], c->st));
     WTD_TRY(wtd_cuerr(cudaStreamSynchronize(c->st)));
     w->timed_r = true;
-    /* the context is again what the forward left (the final checkpoint was restored) */
-    w->mark_launches = c->launches;
-    w->mark_mut = c->mut;
     return WTD_OK;
 }
 

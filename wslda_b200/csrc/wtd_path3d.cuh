@@ -63,8 +63,15 @@ template <typename TC> struct PlaneSmem {
     static constexpr size_t plane = (size_t)(NY) * PlaneGeo::PITCH * sizeof(C);
     static constexpr size_t scr = (size_t)PlaneGeo::SCR * sizeof(C);
     static constexpr size_t tab = (sizeof(LineTab<TC, WTD_L_NMAX>) + 15) / 16 * 16;
-    /* k3_plane_h: table, psi plane, K plane, team scratch */
-    static constexpr size_t h_bytes = tab + 2 * plane + scr;
+    /* k3_plane_h: table, the CTA's coefficient planes (compute precision, plane layout:
+     * variable mass alpha, A_y, A_z and the kinetic coefficient of the component; constant
+     * mass the kinetic coefficient), then per state in flight a psi plane, a K plane and the
+     * team scratch.  Two states per CTA where that still leaves two CTAs per SM. */
+    static constexpr int NCF = WTD_VAR ? 4 : 1;
+    static constexpr size_t cfp = ((size_t)NCF * (NY) * PlaneGeo::PITCH * sizeof(TC) + 15) / 16 * 16;
+    static constexpr size_t hstate = 2 * plane + scr;
+    static constexpr int HS = (tab + cfp + 2 * hstate) * 2 + 2048 <= WTD_SMEM_MAX ? 2 : 1;
+    static constexpr size_t h_bytes = tab + cfp + (size_t)HS * hstate;
     /* k3_plane_dens: table, psi plane, team scratch, three FP64 accumulators */
     static constexpr size_t d_bytes = tab + plane + scr + 3 * (size_t)WTD_L_NYZ * sizeof(double);
 };
@@ -73,23 +80,22 @@ template <typename TC> struct PlaneSmem {
 template <int n, int T, typename TC, bool VAR>
 __device__ __forceinline__ void plane_h_axis(const typename cplx<TC>::t *P, typename cplx<TC>::t *Kp,
                                             typename cplx<TC>::t *scr, const LineTab<TC, WTD_L_NMAX> &Tb, int ax,
-                                            int g, int line, const double *cf, int pb, int comp, bool first)
+                                            int g, int line, const TC *cfs, int comp, bool first)
 {
     typedef typename cplx<TC>::t C;
     constexpr int n1 = n / T, PITCH = PlaneGeo::PITCH;
     const bool yl = ax == 1;
     /* smem index and lattice index of slice point i (the line coordinate is g + T i) */
     auto at = [&](int i) -> int { const int c = g + T * i; return yl ? c * PITCH + line : line * PITCH + c; };
-    auto pt = [&](int i) -> int { const int c = g + T * i; return pb + (yl ? c * NZ + line : line * NZ + c); };
+    constexpr int PL = (NY) * PITCH;                   /* one coefficient plane */
     const TC *lapk = Tb.lapk[ax], *dk = Tb.dk[ax];
     const C *tw = Tb.tw[ax];
     const TC sgn = comp ? (TC)-1 : (TC)1;
     C v[n1], w[n1];
     if (VAR) {
-        const int alc = comp ? CF_ALB : CF_ALA;
 #pragma unroll
         for (int i = 0; i < n1; i++) {
-            const TC al = (TC)CFP(alc, pt(i));
+            const TC al = cfs[at(i)];
             v[i] = P[at(i)];
             v[i].x *= al; v[i].y *= al;
         }
@@ -116,7 +122,6 @@ __device__ __forceinline__ void plane_h_axis(const typename cplx<TC>::t *P, type
     if (VAR) {
 #pragma unroll
         for (int i = 0; i < n1; i++) w[i] = v[i];
-        const int Ac = (comp ? CF_ABX : CF_AAX) + ax;
         team_mul_d<n, T>(w, dk, g);
         team_inv<n, T>(w, scr, g, tw);
         C hk[n1];
@@ -124,7 +129,7 @@ __device__ __forceinline__ void plane_h_axis(const typename cplx<TC>::t *P, type
         for (int i = 0; i < n1; i++) hk[i] = Kp[at(i)];
 #pragma unroll
         for (int i = 0; i < n1; i++) {
-            const TC A = (TC)CFP(Ac, pt(i));
+            const TC A = cfs[ax * PL + at(i)];
             C h = hk[i];
             h.x += A * w[i].y; h.y += -A * w[i].x;
             Kp[at(i)] = h;
@@ -132,7 +137,6 @@ __device__ __forceinline__ void plane_h_axis(const typename cplx<TC>::t *P, type
     }
     team_mul_lap<n, T>(v, lapk, g);
     team_inv<n, T>(v, scr, g, tw);
-    const int aco = comp ? CF_AB : CF_AA;
     C hk[n1];
 #pragma unroll
     for (int i = 0; i < n1; i++) {
@@ -140,7 +144,7 @@ __device__ __forceinline__ void plane_h_axis(const typename cplx<TC>::t *P, type
     }
 #pragma unroll
     for (int i = 0; i < n1; i++) {
-        const TC a = sgn * (TC)CFP(aco, pt(i));
+        const TC a = sgn * cfs[(VAR ? 3 : 0) * PL + at(i)];
         C h = hk[i];
         h.x += a * v[i].x; h.y += a * v[i].y;
         Kp[at(i)] = h;
@@ -151,52 +155,63 @@ __device__ __forceinline__ void plane_h_axis(const typename cplx<TC>::t *P, type
  * k3_plane_h
  * -------------------------------------------------------------------------------------*/
 template <typename TY, typename TC, bool VAR>
-__global__ void __launch_bounds__(PlaneGeo::PT) k3_plane_h(const TY *__restrict__ Y, typename cplx<TC>::t *__restrict__ K,
-                                                          const double *__restrict__ cf, int S, const double2 *gtw,
-                                                          const double *gk)
+__global__ void __launch_bounds__(PlaneGeo::PT * PlaneSmem<TC>::HS) k3_plane_h(const TY *__restrict__ Y,
+                                                                             typename cplx<TC>::t *__restrict__ K,
+                                                                             const double *__restrict__ cf, int S,
+                                                                             const double2 *gtw, const double *gk)
 {
     typedef typename cplx<TC>::t C;
     typedef PlaneSmem<TC> SM;
     typedef PlaneGeo PG;
-    constexpr int N = WTD_NUMEL, NYZ = WTD_L_NYZ, PT = PG::PT, PITCH = PG::PITCH;
+    constexpr int N = WTD_NUMEL, NYZ = WTD_L_NYZ, PT = PG::PT, PITCH = PG::PITCH, HS = SM::HS, PL = (NY) * PITCH;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LineTab<TC, WTD_L_NMAX> &Tb = *(LineTab<TC, WTD_L_NMAX> *)smem_raw;
-    C *P = (C *)(smem_raw + SM::tab);
-    C *Kp = P + (NY) * PITCH;
-    C *Sc = Kp + (NY) * PITCH;
+    TC *CFs = (TC *)(smem_raw + SM::tab);
+    /* this CTA's (component, x-plane) pair, the same for every state it processes; its states
+     * are chunk, chunk + nch, ... split over the HS halves of the CTA */
+    const int pairs = 2 * NX, pr = (int)(blockIdx.x % pairs), chunk = (int)(blockIdx.x / pairs);
+    const int nch = (int)(gridDim.x / pairs);
+    const int comp = pr / NX, x = pr - comp * NX;
+    const int half = threadIdx.x / PT, t = threadIdx.x - half * PT;
+    C *P = (C *)(smem_raw + SM::tab + SM::cfp + (size_t)half * SM::hstate);
+    C *Kp = P + PL;
+    C *Sc = Kp + PL;
     line_tables<TC, WTD_L_NMAX, NX, NY, NZ>(Tb, gtw, gk, WTD_KT);
+    /* the pair's coefficients, once per launch */
+    for (int k = 0; k < SM::NCF; k++) {
+        const int cfk = VAR ? (k == 0 ? CF_ALA + comp : k == 1 ? (comp ? CF_ABY : CF_AAY) : k == 2 ? (comp ? CF_ABZ : CF_AAZ)
+                                                                                          : CF_AA + comp)
+                            : CF_AA + comp;
+        const double *src = cf + (size_t)cfk * N + (size_t)x * NYZ;
+        for (int i = threadIdx.x; i < NYZ; i += blockDim.x) CFs[k * PL + (i / NZ) * PITCH + (i % NZ)] = (TC)src[i];
+    }
     __syncthreads();
-    const int t = threadIdx.x;
-    const size_t items = (size_t)2 * S * NX;
-    for (size_t b = blockIdx.x; b < items; b += gridDim.x) {
-        const int f = (int)(b / NX), x = (int)(b - (size_t)f * NX);
-        const int comp = f >= S ? 1 : 0;
-        const size_t base = (size_t)f * N + (size_t)x * NYZ;   /* the plane's first point */
+    for (int n0 = HS * chunk; n0 < S; n0 += HS * nch) {
+        const int n = n0 + half;
+        const bool act = n < S;                          /* uniform per half (whole warps) */
+        const size_t base = ((size_t)comp * S + n) * N + (size_t)x * NYZ;   /* the plane's first point */
         const LineTab<TC, WTD_L_NMAX> &T = *opaque_ptr(&Tb);
-        const double *cfi = opaque_ptr(cf);
-        if (t == 0 && b + gridDim.x < items) {
-            const size_t fn = (b + gridDim.x) / NX, xn = (b + gridDim.x) - fn * NX;
-            prefetch_l2(Y + fn * N + xn * NYZ, (size_t)NYZ * sizeof(TY));
-        }
-        for (int i = t; i < NYZ; i += PT) {
-            const double2 a = to_d(Y[base + i]);
-            C c; c.x = (TC)a.x; c.y = (TC)a.y;
-            P[(i / NZ) * PITCH + (i % NZ)] = c;
-        }
+        const TC *cfs = opaque_ptr((const TC *)CFs);
+        if (t == 0 && act && n + HS * nch < S) prefetch_l2(Y + base + (size_t)HS * nch * N, (size_t)NYZ * sizeof(TY));
+        if (act)
+            for (int i = t; i < NYZ; i += PT) {
+                const double2 a = to_d(Y[base + i]);
+                C c; c.x = (TC)a.x; c.y = (TC)a.y;
+                P[(i / NZ) * PITCH + (i % NZ)] = c;
+            }
         __syncthreads();
-        if (t < PG::AY) {
+        if (act && t < PG::AY) {
             const int line = t / PG::TY, g = t - line * PG::TY;
-            plane_h_axis<NY, PG::TY, TC, VAR>(P, Kp, Sc + line * Team<NY, PG::TY>::scratch, T, 1, g, line, cfi,
-                                              x * NYZ, comp, true);
+            plane_h_axis<NY, PG::TY, TC, VAR>(P, Kp, Sc + line * Team<NY, PG::TY>::scratch, T, 1, g, line, cfs, comp, true);
         }
         __syncthreads();
-        if (t < PG::AZ) {
+        if (act && t < PG::AZ) {
             const int line = t / PG::TZ, g = t - line * PG::TZ;
-            plane_h_axis<NZ, PG::TZ, TC, VAR>(P, Kp, Sc + line * Team<NZ, PG::TZ>::scratch, T, 2, g, line, cfi,
-                                              x * NYZ, comp, false);
+            plane_h_axis<NZ, PG::TZ, TC, VAR>(P, Kp, Sc + line * Team<NZ, PG::TZ>::scratch, T, 2, g, line, cfs, comp, false);
         }
         __syncthreads();
-        for (int i = t; i < NYZ; i += PT) K[base + i] = Kp[(i / NZ) * PITCH + (i % NZ)];
+        if (act)
+            for (int i = t; i < NYZ; i += PT) K[base + i] = Kp[(i / NZ) * PITCH + (i % NZ)];
         __syncthreads();
     }
 }
@@ -219,20 +234,37 @@ template <typename TC, int CL, int TX_, int HPAD> struct XSmem {
     static constexpr int HP = NX + HPAD;                                    /* padded line of H */
     static constexpr size_t tab = (sizeof(LineTab<TC, WTD_L_NMAX>) + 15) / 16 * 16;
     static constexpr size_t hs = (size_t)LINES * HP * sizeof(C);            /* H, then the update, per line */
+    /* the state's values per line (teams of TX > 1 threads; a thread that owns a whole line
+     * reads its values from L2/L1 instead) */
+    static constexpr bool YS = TX > 1;
+    static constexpr size_t ys = YS ? hs : 0;
     static constexpr size_t scr = (size_t)LINES * team_scratch(NX, TX) * sizeof(C);
     static constexpr size_t red = 80 * sizeof(double);
-    static constexpr size_t base = tab + hs + scr + red;
+    static constexpr size_t base = tab + hs + ys + scr + red;
     /* FP64 slabs of the local-term coefficients at this CTA's columns, loaded once per launch
      * (the coefficients are the same for every state): DRE, DIM, V_a, V_b and, with variable
-     * mass, N_a, N_b, CJ_a, CJ_b — as many of these as fit beside the rest (8, 4 or none);
+     * mass, N_a, N_b, CJ_a, CJ_b — as many of these as fit beside the rest, in this order;
      * rows of CP doubles, padded so that the 16 lanes of a half warp (4 x-rows of 4 columns)
      * fall on distinct banks */
     static constexpr int CP = QC + 4;
     static constexpr size_t slab = (size_t)NX * CP * sizeof(double);
-    static constexpr int NCW = WTD_VAR ? 8 : 4;
-    static constexpr int NCS = base + (size_t)NCW * slab + 64 <= WTD_SMEM_MAX ? NCW
-                             : base + 4 * slab + 64 <= WTD_SMEM_MAX ? 4 : 0;
-    static constexpr size_t bytes = base + (size_t)NCS * slab;
+    /* and slabs in the compute precision of the coefficients the transforms' terms use in that
+     * precision anyway — the kinetic coefficient and alpha of each component (AA_a, AA_b, then
+     * with variable mass AL_a, AL_b) — rows of CPT (a half warp's 4 x-rows of 8 columns on
+     * distinct banks).  Preference, whole pairs of components only: DRE, DIM, V_a, V_b; then the
+     * compute-precision slabs; then N_a, N_b, CJ_a, CJ_b. */
+    static constexpr int CPT = QC + 8;
+    static constexpr size_t tslab = (size_t)NX * CPT * sizeof(TC);
+    static constexpr size_t room = base + 64 > WTD_SMEM_MAX ? 0 : WTD_SMEM_MAX - 64 - base;
+    static constexpr int NCW = WTD_VAR ? 8 : 4, NTW = WTD_VAR ? 4 : 2;
+    static constexpr int NC1 = (int)(room / slab) >= 4 ? 4 : (int)(room / slab) / 2 * 2;
+    static constexpr size_t room1 = room - (size_t)NC1 * slab;
+    static constexpr int NTS = NC1 < 4 ? 0 : ((int)(room1 / tslab) >= NTW ? NTW : (int)(room1 / tslab) / 2 * 2);
+    static constexpr size_t room2 = room1 - (size_t)NTS * tslab;
+    static constexpr int NC2 = (NC1 < 4 || NCW == 4) ? 0 : ((int)(room2 / slab) >= 4 ? 4 : (int)(room2 / slab) / 2 * 2);
+    static constexpr int NCS = NC1 + NC2;
+    static constexpr size_t base2 = base + (size_t)NCS * slab;
+    static constexpr size_t bytes = base2 + (size_t)NTS * tslab;
     static constexpr bool ok = WTD_L_NYZ % CL == 0 && XT <= 1024 && XT % 32 == 0 && NX % (TX * TX) == 0;
 };
 
@@ -241,6 +273,8 @@ __device__ __forceinline__ int xslab_cf(int k)
 {
     return k == 0 ? CF_DRE : k == 1 ? CF_DIM : k < 4 ? CF_VA + (k - 2) : k < 6 ? CF_NA + (k - 4) : CF_CJA + (k - 6);
 }
+/* the CF_* list entry of compute-precision slab k: AA_a, AA_b, then (variable mass) AL_a, AL_b */
+__device__ __forceinline__ int xtslab_cf(int k) { return k < 2 ? CF_AA + k : CF_ALA + (k - 2); }
 
 /* Sum over the cluster of one double per thread, in two halves.  cluster_post adds the CTA's
  * values (warp sums, then warp 0 over the warp sums — the order of block_sum), publishes the
@@ -288,11 +322,15 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
     const StepArgs &a = xa.s;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LineTab<TC, WTD_L_NMAX> &Tb = *(LineTab<TC, WTD_L_NMAX> *)smem_raw;
+    static_assert(sizeof(TY) == sizeof(typename cplx<TC>::t), "states stored in the compute precision");
     C *Hs = (C *)(smem_raw + SM::tab);                 /* [line][HP] */
-    C *Scr = Hs + SM::LINES * HP;                      /* [line][team scratch] */
-    double *red = (double *)(smem_raw + SM::tab + SM::hs + SM::scr);
+    C *Ysm = Hs + SM::LINES * HP;                      /* [line][HP]: the state of the iteration */
+    C *Scr = Ysm + SM::LINES * HP;                     /* [line][team scratch] */
+    double *red = (double *)(smem_raw + SM::tab + SM::hs + SM::ys + SM::scr);
     double *cs = (double *)(smem_raw + SM::base);        /* [NCS][NX][CP] coefficient slabs */
     constexpr int NCS = SM::NCS, CP = SM::CP, SL = NX * CP;
+    TC *ct = (TC *)(smem_raw + SM::base2);               /* [NTS][NX][CPT] compute-precision slabs */
+    constexpr int NTS = SM::NTS, CPT = SM::CPT, STL = NX * CPT;
     __shared__ double cred[2];
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
@@ -303,6 +341,9 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
     const int q = rank * QC + j;                        /* this team's (y, z) column */
     C *scr = Scr + line * Team<NX, TX>::scratch;
     C *Hl = Hs + line * HP;                             /* this line's H */
+    C *Yl = Ysm + line * HP;                            /* this line's state values */
+    const C *Yo = Ysm + (comp ? line - QC : line + QC) * HP;   /* the other component's, same column */
+    constexpr bool YS = SM::YS;
     const TC sgn = comp ? (TC)-1 : (TC)1;
     TY *Y = (TY *)a.y;
     TY *YO = a.yout ? (TY *)a.yout : Y;
@@ -323,6 +364,13 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
         for (int i = t; i < NX * QC; i += XT) {
             const int x = i / QC, jj = i - x * QC;
             cs[k * SL + x * CP + jj] = src[(size_t)x * NYZ + jj];
+        }
+    }
+    for (int k = 0; k < NTS; k++) {
+        const double *src = a.cf + (size_t)xtslab_cf(k) * N + rank * QC;
+        for (int i = t; i < NX * QC; i += XT) {
+            const int x = i / QC, jj = i - x * QC;
+            ct[k * STL + x * CPT + jj] = (TC)src[(size_t)x * NYZ + jj];
         }
     }
     __syncthreads();
@@ -358,16 +406,44 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
         const C *tw = T.tw[0];
         const double *cf = opaque_ptr(a.cf);
         const size_t fb = (comp ? SN : 0) + (size_t)n * N;     /* this component of state n */
-        const size_t ub = (size_t)n * N, vb = SN + (size_t)n * N;
+        const size_t ob = (comp ? 0 : SN) + (size_t)n * N;     /* the other component */
+        /* state values at x of this line and of the other component's line at this column */
+        auto yown = [&](int x) -> C {
+            if (YS) return Yl[x];
+            const double2 d = to_d(Y[fb + (size_t)x * NYZ + q]);
+            C c; c.x = (TC)d.x; c.y = (TC)d.y;
+            return c;
+        };
+        auto yoth = [&](int x) -> C {
+            if (YS) return Yo[x];
+            const double2 d = to_d(Y[ob + (size_t)x * NYZ + q]);
+            C c; c.x = (TC)d.x; c.y = (TC)d.y;
+            return c;
+        };
         const bool haveH = (PASS == 1) || (PASS == 3) || (PASS == 0 && !a.fk_given);
         double E = 0.0;
         int eslot = 0;
+        /* this line's state values into shared memory (read once from HBM; the local terms of
+         * the other component's line read them there too), and K_yz into the line's H */
+#pragma unroll
+        for (int i = 0; i < n1; i++) {
+            const int x = g + TX * i, p = x * NYZ + q;
+            if (YS) {
+                const double2 yd = to_d(Y[fb + p]);
+                C c; c.x = (TC)yd.x; c.y = (TC)yd.y;
+                Yl[x] = c;
+            }
+            if (haveH) Hl[x] = Kin[fb + p];
+        }
+        __syncthreads();
         if (haveH) {
             /* K_yz plus the local terms (pca_kernels.cu:233-391) at this thread's points */
 #pragma unroll 2
             for (int i = 0; i < n1; i++) {
                 const int x = g + TX * i, p = x * NYZ + q;
-                const double2 u = to_d(Y[ub + p]), v = to_d(Y[vb + p]);
+                const C cs0 = yown(x), cs1 = yoth(x);
+                const C cu = comp ? cs1 : cs0, cv = comp ? cs0 : cs1;
+                const double2 u = make_double2((double)cu.x, (double)cu.y), v = make_double2((double)cv.x, (double)cv.y);
                 /* this component's coefficients: from the slabs, else from L2 */
                 auto co = [&](int k) -> double {
                     return k < NCS ? cs[k * SL + x * CP + j] : ld_ro_keep(cf + (size_t)xslab_cf(k) * N + p, pol);
@@ -392,7 +468,7 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
                         h.y = -vs * v.y + (dr * u.y - di * u.x);
                     }
                 }
-                const C k = Kin[fb + p];
+                const C k = Hl[x];
                 C r; r.x = (TC)(h.x + (double)k.x); r.y = (TC)(h.y + (double)k.y);
                 Hl[x] = r;
             }
@@ -403,9 +479,10 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
 #pragma unroll
                 for (int i = 0; i < n1; i++) {
                     const int p = (g + TX * i) * NYZ + q;
-                    const double2 y = to_d(Y[fb + p]);
-                    const TC al = (TC)ld_ro_keep(cf + (size_t)alc * N + p, pol);
-                    v[i].x = (TC)y.x * al; v[i].y = (TC)y.y * al;
+                    const C y = yown(g + TX * i);
+                    const TC al = (2 + comp < NTS) ? ct[(2 + comp) * STL + (g + TX * i) * CPT + j]
+                                                   : (TC)ld_ro_keep(cf + (size_t)alc * N + p, pol);
+                    v[i].x = y.x * al; v[i].y = y.y * al;
                 }
                 team_fwd<NX, TX>(v, scr, g, tw);
                 team_mul_lap<NX, TX>(v, lapk, g);
@@ -417,10 +494,7 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
                 }
             }
 #pragma unroll
-            for (int i = 0; i < n1; i++) {
-                const double2 y = to_d(Y[fb + (g + TX * i) * NYZ + q]);
-                v[i].x = (TC)y.x; v[i].y = (TC)y.y;
-            }
+            for (int i = 0; i < n1; i++) v[i] = yown(g + TX * i);
             team_fwd<NX, TX>(v, scr, g, tw);
             if (VAR) {
                 const int Ac = comp ? CF_ABX : CF_AAX;
@@ -443,12 +517,12 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
 #pragma unroll
             for (int i = 0; i < n1; i++) {
                 const int x = g + TX * i, p = x * NYZ + q;
-                const TC ac = sgn * (TC)ld_ro_keep(cf + (size_t)aco * N + p, pol);
+                const TC ac = sgn * ((comp < NTS) ? ct[comp * STL + x * CPT + j] : (TC)ld_ro_keep(cf + (size_t)aco * N + p, pol));
                 C h = Hl[x];
                 h.x += ac * v[i].x; h.y += ac * v[i].y;
                 Hl[x] = h;
-                const double2 y = to_d(Y[fb + p]);
-                e += y.x * (double)h.x + y.y * (double)h.y;
+                const C y = yown(x);
+                e += (double)y.x * (double)h.x + (double)y.y * (double)h.y;
             }
             eslot = ncalls & 1;
             ncalls++;
@@ -459,12 +533,10 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
         constexpr int NR = (PASS == 0) ? NH - 1 : (PASS == 1 ? 1 : 0);
         constexpr int NRP = (PASS == 0) ? (sizeof(TH) == 8 ? 2 : 1) : (PASS == 1 ? 1 : 0);
         auto ring = [&](int k) -> const TH * { return (const TH *)xa.s.slot[PASS == 1 ? NH - 2 : k]; };
-        TY y0r[n1];
         TH frr[NRP > 0 ? NRP : 1][n1];
 #pragma unroll
         for (int i = 0; i < n1; i++) {
             const size_t gi = fb + (size_t)(g + TX * i) * NYZ + q;
-            y0r[i] = Y[gi];
 #pragma unroll
             for (int k = 0; k < NRP; k++) frr[k][i] = ld_stream(ring(k) + gi);
         }
@@ -477,7 +549,8 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
             for (int i = 0; i < n1; i++) {
                 const int x = g + TX * i;
                 const size_t gi = fb + x * NYZ + q;
-                const double2 y0 = to_d(y0r[i]);
+                const C yc = yown(x);
+                const double2 y0 = make_double2((double)yc.x, (double)yc.y);
                 const C h = Hl[x];
                 ((TH *)xa.s.slot[NH - 1])[gi] = from_d<TH>(make_double2((double)h.x - E * y0.x, (double)h.y - E * y0.y));
             }
@@ -490,7 +563,8 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
         for (int i = 0; i < n1; i++) {
             const int x = g + TX * i;
             const size_t gi = fb + x * NYZ + q;
-            const double2 y0 = to_d(y0r[i]);
+            const C yc = yown(x);
+            const double2 y0 = make_double2((double)yc.x, (double)yc.y);
             double2 fr[NR > 0 ? NR : 1], fkg = make_double2(0.0, 0.0);
 #pragma unroll
             for (int k = 0; k < NR; k++) fr[k] = to_d(k < NRP ? frr[k < NRP ? k : 0][i] : ld_stream(ring(k) + gi));
