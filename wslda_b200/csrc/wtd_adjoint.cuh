@@ -90,26 +90,15 @@ __device__ __forceinline__ void lap2(double2 *BU, double2 *BV, const double2 *tw
     fft_inverse<G, 2>(BU, (int)(BV - BU), tw);
 }
 
-/* points of a state per thread of the reverse kernels (512 threads, or one warp-rounded
- * thread per point).  The per-point values a kernel needs again after a block sum stay on the
- * SM — one pair in registers, the others in shared memory (a second pair of field buffers,
- * W) — instead of being read back from L2. */
-template <class G> struct AdjPts {
-    static constexpr int threads = G::ntot >= 512 ? 512 : ((G::ntot + 31) / 32) * 32;
-    static constexpr int npt = (G::ntot + threads - 1) / threads;
-};
-
 /* reverse of pass B (corrector half step), persistent CTAs over states */
 template <class G, int NH>
 __global__ void __launch_bounds__(512, 1) k_adj_B(AdjArgs a, const double2 *gtw, const double *gk)
 {
-    constexpr int N = G::ntot, NPT = AdjPts<G>::npt;
+    constexpr int N = G::ntot;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *BU = (double2 *)smem_raw;
     double2 *BV = BU + G::padded;
-    double2 *WU = BV + G::padded;
-    double2 *WV = WU + G::padded;
-    double2 *tw = WV + G::padded;
+    double2 *tw = BV + G::padded;
     double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + G::twtotal);
     double *red = (double *)(kt + 6);
     load_tables<G>(tw, kt, gtw, gk);
@@ -121,73 +110,52 @@ __global__ void __launch_bounds__(512, 1) k_adj_B(AdjArgs a, const double2 *gtw,
         const size_t bu = (size_t)n * N, bv = SN + bu;
         const double cn = (1.0 - 2.0 * a.occ[n]) * 0.5 * a.wcnt[n] * a.inv_lperp;
         const double kp2 = a.kp2[n];
-        /* per point of this thread: y1, then y_p (registers); ybar (BU, BV), then Pbar (WU, WV) */
-        double2 yu[NPT], yv[NPT];
         /* ybar_{k+1} (+ the pending density adjoint of nu(y_{k+1})), r1 = Re<ybar, y1> */
         double r1 = 0.0;
-#pragma unroll
-        for (int k = 0; k < NPT; k++) {
-            const int p = threadIdx.x + k * blockDim.x;
-            if (p < N) {
-                double2 u = a.y1[bu + p], v = a.y1[bv + p], gu = a.ybar[bu + p], gv = a.ybar[bv + p];
-                if (a.nubar) nu_adjoint(gu, gv, a.nubar[p], cn, u, v);
-                yu[k] = u; yv[k] = v;
-                BU[G::off(p)] = gu;
-                BV[G::off(p)] = gv;
-                r1 += gu.x * u.x + gu.y * u.y + gv.x * v.x + gv.y * v.y;
-            }
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            double2 u = a.y1[bu + p], v = a.y1[bv + p], gu = a.ybar[bu + p], gv = a.ybar[bv + p];
+            if (a.nubar) nu_adjoint(gu, gv, a.nubar[p], cn, u, v);
+            BU[G::off(p)] = gu;
+            BV[G::off(p)] = gv;
+            r1 += gu.x * u.x + gu.y * u.y + gv.x * v.x + gv.y * v.y;
         }
         r1 = block_sum(r1, red);
         const double inv_n = 1.0 / a.nrm[n];
         /* Pbar = yhbar = (ybar - dV r1 y1)/n;  fbar_p = i dt c Pbar;  s = Re<fbar_p, y_p> */
         double s = 0.0;
-#pragma unroll
-        for (int k = 0; k < NPT; k++) {
-            const int p = threadIdx.x + k * blockDim.x;
-            if (p < N) {
-                const int o = G::off(p);
-                const double2 gu = BU[o], gv = BV[o], u = yu[k], v = yv[k];
-                const double2 qu = make_double2((gu.x - dV * r1 * u.x) * inv_n, (gu.y - dV * r1 * u.y) * inv_n);
-                const double2 qv = make_double2((gv.x - dV * r1 * v.x) * inv_n, (gv.y - dV * r1 * v.y) * inv_n);
-                a.pbar[bu + p] = qu;
-                a.pbar[bv + p] = qv;
-                WU[o] = qu; WV[o] = qv;
-                const double2 ypu = a.yp[bu + p], ypv = a.yp[bv + p];
-                yu[k] = ypu; yv[k] = ypv;
-                s += (-dc * qu.y) * ypu.x + (dc * qu.x) * ypu.y + (-dc * qv.y) * ypv.x + (dc * qv.x) * ypv.y;
-            }
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            const int o = G::off(p);
+            double2 u = a.y1[bu + p], v = a.y1[bv + p], gu = BU[o], gv = BV[o];
+            double2 pu = make_double2((gu.x - dV * r1 * u.x) * inv_n, (gu.y - dV * r1 * u.y) * inv_n);
+            double2 pv = make_double2((gv.x - dV * r1 * v.x) * inv_n, (gv.y - dV * r1 * v.y) * inv_n);
+            a.pbar[bu + p] = pu;
+            a.pbar[bv + p] = pv;
+            double2 yu = a.yp[bu + p], yv = a.yp[bv + p];
+            s += (-dc * pu.y) * yu.x + (dc * pu.x) * yu.y + (-dc * pv.y) * yv.x + (dc * pv.x) * yv.y;
         }
         s = block_sum(s, red);
         /* x = fbar_p - 2 s dV y_p, its laplacian in shared memory */
-#pragma unroll
-        for (int k = 0; k < NPT; k++) {
-            const int p = threadIdx.x + k * blockDim.x;
-            if (p < N) {
-                const int o = G::off(p);
-                const double2 qu = WU[o], qv = WV[o], ypu = yu[k], ypv = yv[k];
-                BU[o] = make_double2(-dc * qu.y - 2.0 * s * dV * ypu.x, dc * qu.x - 2.0 * s * dV * ypu.y);
-                BV[o] = make_double2(-dc * qv.y - 2.0 * s * dV * ypv.x, dc * qv.x - 2.0 * s * dV * ypv.y);
-            }
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            const int o = G::off(p);
+            double2 pu = a.pbar[bu + p], pv = a.pbar[bv + p], yu = a.yp[bu + p], yv = a.yp[bv + p];
+            BU[o] = make_double2(-dc * pu.y - 2.0 * s * dV * yu.x, dc * pu.x - 2.0 * s * dV * yu.y);
+            BV[o] = make_double2(-dc * pv.y - 2.0 * s * dV * yv.x, dc * pv.x - 2.0 * s * dV * yv.y);
         }
         lap2<G>(BU, BV, tw, kt);
         const double E = a.E[n];
-#pragma unroll
-        for (int k = 0; k < NPT; k++) {
-            const int p = threadIdx.x + k * blockDim.x;
-            if (p < N) {
-                const int o = G::off(p);
-                const double2 qu = WU[o], qv = WV[o], ypu = yu[k], ypv = yv[k];
-                double2 fu = make_double2(-dc * qu.y, dc * qu.x), fv = make_double2(-dc * qv.y, dc * qv.x);
-                double2 xu = make_double2(fu.x - 2.0 * s * dV * ypu.x, fu.y - 2.0 * s * dV * ypu.y);
-                double2 xv = make_double2(fv.x - 2.0 * s * dV * ypv.x, fv.y - 2.0 * s * dV * ypv.y);
-                double2 hu, hv;
-                h_apply_point(a.cf, N, p, kp2, xu, xv, BU[o], BV[o], hu, hv);
-                a.ypbar[bu + p] = make_double2(hu.x - E * fu.x, hu.y - E * fu.y);
-                a.ypbar[bv + p] = make_double2(hv.x - E * fv.x, hv.y - E * fv.y);
-                double2 wu = make_double2(fu.x - s * dV * ypu.x, fu.y - s * dV * ypu.y);
-                double2 wv = make_double2(fv.x - s * dV * ypv.x, fv.y - s * dV * ypv.y);
-                field_adjoint(ds, N, p, wu, wv, ypu, ypv);
-            }
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            const int o = G::off(p);
+            double2 pu = a.pbar[bu + p], pv = a.pbar[bv + p], yu = a.yp[bu + p], yv = a.yp[bv + p];
+            double2 fu = make_double2(-dc * pu.y, dc * pu.x), fv = make_double2(-dc * pv.y, dc * pv.x);
+            double2 xu = make_double2(fu.x - 2.0 * s * dV * yu.x, fu.y - 2.0 * s * dV * yu.y);
+            double2 xv = make_double2(fv.x - 2.0 * s * dV * yv.x, fv.y - 2.0 * s * dV * yv.y);
+            double2 hu, hv;
+            h_apply_point(a.cf, N, p, kp2, xu, xv, BU[o], BV[o], hu, hv);
+            a.ypbar[bu + p] = make_double2(hu.x - E * fu.x, hu.y - E * fu.y);
+            a.ypbar[bv + p] = make_double2(hv.x - E * fv.x, hv.y - E * fv.y);
+            double2 wu = make_double2(fu.x - s * dV * yu.x, fu.y - s * dV * yu.y);
+            double2 wv = make_double2(fv.x - s * dV * yv.x, fv.y - s * dV * yv.y);
+            field_adjoint(ds, N, p, wu, wv, yu, yv);
         }
         __syncthreads();
     }
@@ -199,13 +167,11 @@ template <class G, int NH>
 __global__ void __launch_bounds__(512, 1) k_adj_A(AdjArgs a, const double2 *gtw, const double *gk)
 {
     typedef Abm<NH> AB;
-    constexpr int N = G::ntot, NPT = AdjPts<G>::npt;
+    constexpr int N = G::ntot;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *BU = (double2 *)smem_raw;
     double2 *BV = BU + G::padded;
-    double2 *WU = BV + G::padded;
-    double2 *WV = WU + G::padded;
-    double2 *tw = WV + G::padded;
+    double2 *tw = BV + G::padded;
     double (*kt)[WTD_KT] = (double (*)[WTD_KT])(tw + G::twtotal);
     double *red = (double *)(kt + 6);
     load_tables<G>(tw, kt, gtw, gk);
@@ -218,89 +184,66 @@ __global__ void __launch_bounds__(512, 1) k_adj_A(AdjArgs a, const double2 *gtw,
         const size_t bu = (size_t)n * N, bv = SN + bu;
         const double cn = (1.0 - 2.0 * a.occ[n]) * 0.5 * a.wcnt[n] * a.inv_lperp;
         const double kp2 = a.kp2[n];
-        /* per point of this thread: y_pred, then y_k (registers); ybar_pred (BU, BV), then
-         * fbar_k (WU, WV) */
-        double2 yu[NPT], yv[NPT];
         /* ybar_pred (+ density adjoint of nu(y_pred)), r2 = Re<ybar_pred, y_pred> */
         double r2 = 0.0;
-#pragma unroll
-        for (int k = 0; k < NPT; k++) {
-            const int p = threadIdx.x + k * blockDim.x;
-            if (p < N) {
-                double2 u = a.yp[bu + p], v = a.yp[bv + p], g0 = a.ypbar[bu + p], g1 = a.ypbar[bv + p];
-                if (a.nubar) nu_adjoint(g0, g1, a.nubar[p], cn, u, v);
-                yu[k] = u; yv[k] = v;
-                BU[G::off(p)] = g0;
-                BV[G::off(p)] = g1;
-                r2 += g0.x * u.x + g0.y * u.y + g1.x * v.x + g1.y * v.y;
-            }
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            double2 u = a.yp[bu + p], v = a.yp[bv + p], gu = a.ypbar[bu + p], gv = a.ypbar[bv + p];
+            if (a.nubar) nu_adjoint(gu, gv, a.nubar[p], cn, u, v);
+            BU[G::off(p)] = gu;
+            BV[G::off(p)] = gv;
+            r2 += gu.x * u.x + gu.y * u.y + gv.x * v.x + gv.y * v.y;
         }
         r2 = block_sum(r2, red);
         const double inv_n = 1.0 / a.nrm[n];
         /* ytbar = (ybar_pred - dV r2 y_pred)/n;  ybar_k = ytbar + Pbar;
          * fbar_{k-j} += i dt (b_j ytbar + a_j Pbar);  s = Re<fbar_k, y_k> */
         double s = 0.0;
+        for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            const int o = G::off(p);
 #pragma unroll
-        for (int k = 0; k < NPT; k++) {
-            const int p = threadIdx.x + k * blockDim.x;
-            if (p < N) {
-                const int o = G::off(p);
+            for (int comp = 0; comp < 2; comp++) {
+                const size_t gi = (comp ? bv : bu) + p;
+                const double2 y = a.yp[gi], g = comp ? BV[o] : BU[o], P = a.pbar[gi];
+                const double2 t = make_double2((g.x - dV * r2 * y.x) * inv_n, (g.y - dV * r2 * y.y) * inv_n);
+                a.ybar[gi] = make_double2(t.x + P.x, t.y + P.y);
 #pragma unroll
-                for (int comp = 0; comp < 2; comp++) {
-                    const size_t gi = (comp ? bv : bu) + p;
-                    const double2 y = comp ? yv[k] : yu[k], g = comp ? BV[o] : BU[o], P = a.pbar[gi];
-                    const double2 t = make_double2((g.x - dV * r2 * y.x) * inv_n, (g.y - dV * r2 * y.y) * inv_n);
-                    a.ybar[gi] = make_double2(t.x + P.x, t.y + P.y);
-                    double2 f0 = make_double2(0.0, 0.0);
-#pragma unroll
-                    for (int j = 0; j < NH; j++) {
-                        const double cb = AB::b(j), ca = (j < AB::na) ? AB::a(j) : 0.0;
-                        const double zx = cb * t.x + ca * P.x, zy = cb * t.y + ca * P.y;
-                        double2 f = a.fring[j][gi];
-                        f.x -= dt * zy;
-                        f.y += dt * zx;
-                        a.fring[j][gi] = f;
-                        if (j == 0) f0 = f;
-                    }
-                    if (a.has_h) {
+                for (int j = 0; j < NH; j++) {
+                    const double cb = AB::b(j), ca = (j < AB::na) ? AB::a(j) : 0.0;
+                    const double zx = cb * t.x + ca * P.x, zy = cb * t.y + ca * P.y;
+                    double2 f = a.fring[j][gi];
+                    f.x -= dt * zy;
+                    f.y += dt * zx;
+                    a.fring[j][gi] = f;
+                    if (j == 0 && a.has_h) {
                         const double2 yk = a.y1[gi];
-                        s += f0.x * yk.x + f0.y * yk.y;
-                        if (comp) { yv[k] = yk; WV[o] = f0; } else { yu[k] = yk; WU[o] = f0; }
+                        s += f.x * yk.x + f.y * yk.y;
                     }
                 }
             }
         }
         if (a.has_h) {
             s = block_sum(s, red);
-#pragma unroll
-            for (int k = 0; k < NPT; k++) {
-                const int p = threadIdx.x + k * blockDim.x;
-                if (p < N) {
-                    const int o = G::off(p);
-                    const double2 fu = WU[o], fv = WV[o], ku = yu[k], kv = yv[k];
-                    BU[o] = make_double2(fu.x - 2.0 * s * dV * ku.x, fu.y - 2.0 * s * dV * ku.y);
-                    BV[o] = make_double2(fv.x - 2.0 * s * dV * kv.x, fv.y - 2.0 * s * dV * kv.y);
-                }
+            for (int p = threadIdx.x; p < N; p += blockDim.x) {
+                const int o = G::off(p);
+                double2 fu = a.fring[0][bu + p], fv = a.fring[0][bv + p], yu = a.y1[bu + p], yv = a.y1[bv + p];
+                BU[o] = make_double2(fu.x - 2.0 * s * dV * yu.x, fu.y - 2.0 * s * dV * yu.y);
+                BV[o] = make_double2(fv.x - 2.0 * s * dV * yv.x, fv.y - 2.0 * s * dV * yv.y);
             }
             lap2<G>(BU, BV, tw, kt);
             const double E = a.E[n];
-#pragma unroll
-            for (int k = 0; k < NPT; k++) {
-                const int p = threadIdx.x + k * blockDim.x;
-                if (p < N) {
-                    const int o = G::off(p);
-                    const double2 fu = WU[o], fv = WV[o], ku = yu[k], kv = yv[k];
-                    double2 xu = make_double2(fu.x - 2.0 * s * dV * ku.x, fu.y - 2.0 * s * dV * ku.y);
-                    double2 xv = make_double2(fv.x - 2.0 * s * dV * kv.x, fv.y - 2.0 * s * dV * kv.y);
-                    double2 hu, hv;
-                    h_apply_point(a.cf, N, p, kp2, xu, xv, BU[o], BV[o], hu, hv);
-                    double2 g0 = a.ybar[bu + p], g1 = a.ybar[bv + p];
-                    a.ybar[bu + p] = make_double2(g0.x + hu.x - E * fu.x, g0.y + hu.y - E * fu.y);
-                    a.ybar[bv + p] = make_double2(g1.x + hv.x - E * fv.x, g1.y + hv.y - E * fv.y);
-                    double2 wu = make_double2(fu.x - s * dV * ku.x, fu.y - s * dV * ku.y);
-                    double2 wv = make_double2(fv.x - s * dV * kv.x, fv.y - s * dV * kv.y);
-                    field_adjoint(ds, N, p, wu, wv, ku, kv);
-                }
+            for (int p = threadIdx.x; p < N; p += blockDim.x) {
+                const int o = G::off(p);
+                double2 fu = a.fring[0][bu + p], fv = a.fring[0][bv + p], yu = a.y1[bu + p], yv = a.y1[bv + p];
+                double2 xu = make_double2(fu.x - 2.0 * s * dV * yu.x, fu.y - 2.0 * s * dV * yu.y);
+                double2 xv = make_double2(fv.x - 2.0 * s * dV * yv.x, fv.y - 2.0 * s * dV * yv.y);
+                double2 hu, hv;
+                h_apply_point(a.cf, N, p, kp2, xu, xv, BU[o], BV[o], hu, hv);
+                double2 gu = a.ybar[bu + p], gv = a.ybar[bv + p];
+                a.ybar[bu + p] = make_double2(gu.x + hu.x - E * fu.x, gu.y + hu.y - E * fu.y);
+                a.ybar[bv + p] = make_double2(gv.x + hv.x - E * fv.x, gv.y + hv.y - E * fv.y);
+                double2 wu = make_double2(fu.x - s * dV * yu.x, fu.y - s * dV * yu.y);
+                double2 wv = make_double2(fv.x - s * dV * yv.x, fv.y - s * dV * yv.y);
+                field_adjoint(ds, N, p, wu, wv, yu, yv);
             }
         }
         __syncthreads();

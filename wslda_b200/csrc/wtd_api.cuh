@@ -1850,8 +1850,7 @@ static int adj_choose_K(wtd_ctx *c, int nsteps, int K)
 static int adjoint_forward(wtd_ctx *c, int it0, int nsteps, int Kin, const double *mask_h, bool record, double *loss_h)
 {
     constexpr int N = WTD_NUMEL;
-    /* the reverse kernels' shared memory: two pairs of field buffers, tables, block-sum words */
-    constexpr size_t sm = 4 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>) +
+    constexpr size_t sm = 2 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>) +
                           80 * sizeof(double);
     if (sm > WTD_SMEM_MAX) return WTD_ERR_UNSUPPORTED;
     const int K = record ? adj_choose_K(c, nsteps, Kin) : 0;
@@ -1901,8 +1900,7 @@ static int adjoint_reverse(wtd_ctx *c, int nparam, double *grad_h)
     constexpr int N = WTD_NUMEL, NH = WTD_NHIST;
     const int S = c->S;
     const size_t NS = (size_t)2 * S * N;
-    /* the reverse kernels' shared memory: two pairs of field buffers, tables, block-sum words */
-    constexpr size_t sm = 4 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>) +
+    constexpr size_t sm = 2 * (size_t)WG::padded * sizeof(double2) + WG::twtotal * sizeof(double2) + sizeof(KTab<WG>) +
                           80 * sizeof(double);
     AdjWork *w = (AdjWork *)c->adj;
     if (!w || !w->ready || w->mark_launches != c->launches || w->mark_mut != c->mut) return WTD_ERR_STATE;
