@@ -535,24 +535,31 @@ static int staged_step(wtd_ctx *c, bool last)
  * the functional and the coefficients as the fused path does them.
  * -------------------------------------------------------------------------------------*/
 #if CODEDIM == 3
-/* compile-time choice of the x-line kernel's cluster size CL, threads per x-line TX and pad of
- * its H lines: the first candidate that fits one CTA (<= 1024 threads, shared memory): clusters of
- * 16 CTAs before 8, teams of line_team(NX) threads before 2 and 1, a pad of 4 before 1 */
-template <typename TC, int CL, int TX, int HPAD> struct LineFit {
-    static constexpr bool ok = TX >= 1 && XSmem<TC, CL, TX, HPAD>::ok && XSmem<TC, CL, TX, HPAD>::bytes + 64 <= WTD_SMEM_MAX;
+/* compile-time choice of the x-line kernel's cluster size CL, threads per x-line TX, pad of its
+ * H lines and whether it keeps the state's lines in shared memory (YS): the first candidate
+ * that fits one CTA (<= 1024 threads, shared memory) in the order: clusters of 16 CTAs before
+ * 8, teams of line_team(NX) threads before 2 and 1, a pad of 4 before 1, the state's lines in
+ * shared memory before not */
+template <typename TC, int CL, int TX, int HPAD, bool YS> struct LineFit {
+    static constexpr bool ok = TX >= 1 && XSmem<TC, CL, TX, HPAD, YS>::ok &&
+                               XSmem<TC, CL, TX, HPAD, YS>::bytes + 64 <= WTD_SMEM_MAX;
 };
 template <typename TC> struct LineCfg {
     static constexpr int T0 = line_team(NX), T1 = T0 > 2 ? 2 : 1;
-#define WTD_LC(cl, tx, hp) LineFit<TC, cl, tx, hp>::ok
-    static constexpr int k =
-        WTD_LC(16, T0, 4) ? 0 : WTD_LC(16, T0, 1) ? 1 : WTD_LC(8, T0, 4) ? 2 : WTD_LC(8, T0, 1) ? 3 :
-        WTD_LC(16, T1, 4) ? 4 : WTD_LC(16, T1, 1) ? 5 : WTD_LC(8, T1, 4) ? 6 : WTD_LC(8, T1, 1) ? 7 :
-        WTD_LC(16, 1, 4) ? 8 : WTD_LC(16, 1, 1) ? 9 : WTD_LC(8, 1, 4) ? 10 : WTD_LC(8, 1, 1) ? 11 : 12;
-#undef WTD_LC
-    static constexpr int CL = (k % 4 < 2) ? 16 : 8;
-    static constexpr int TX = k < 4 ? T0 : k < 8 ? T1 : 1;
-    static constexpr int HPAD = (k % 2 == 0) ? 4 : 1;
-    static constexpr bool ok = k < 12 && PlaneGeo::ok && PlaneSmem<TC>::h_bytes <= WTD_SMEM_MAX &&
+    /* candidate i: YS = !(i & 1); j = i / 2 gives HPAD (4, 1), CL (16, 16, 8, 8) and TX (T0 for
+     * j < 4, T1 for j < 8, else 1) */
+    static constexpr int cl(int i) { return ((i / 2) % 4 < 2) ? 16 : 8; }
+    static constexpr int tx(int i) { return (i / 2) < 4 ? T0 : (i / 2) < 8 ? T1 : 1; }
+    static constexpr int hp(int i) { return ((i / 2) % 2 == 0) ? 4 : 1; }
+    static constexpr bool ys(int i) { return (i & 1) == 0; }
+    template <int I, bool = (I < 24)> struct Find {
+        static constexpr int value = LineFit<TC, cl(I), tx(I), hp(I), ys(I)>::ok ? I : Find<I + 1>::value;
+    };
+    template <int I> struct Find<I, false> { static constexpr int value = 24; };
+    static constexpr int k = Find<0>::value;
+    static constexpr int CL = cl(k < 24 ? k : 0), TX = tx(k < 24 ? k : 0), HPAD = hp(k < 24 ? k : 0);
+    static constexpr bool YS = ys(k < 24 ? k : 0);
+    static constexpr bool ok = k < 24 && PlaneGeo::ok && PlaneSmem<TC>::h_bytes <= WTD_SMEM_MAX &&
                                PlaneSmem<TC>::d_bytes <= WTD_SMEM_MAX;
 };
 
@@ -567,8 +574,8 @@ template <typename TY, typename TH, typename TC, int PASS, bool GRAD>
 static cudaError_t line_x_attrs()
 {
     typedef LineCfg<TC> L;
-    typedef XSmem<TC, L::CL, L::TX, L::HPAD> SM;
-    auto k = k3_xline<TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD, L::CL, L::TX, L::HPAD>;
+    typedef XSmem<TC, L::CL, L::TX, L::HPAD, L::YS> SM;
+    auto k = k3_xline<TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD, L::CL, L::TX, L::HPAD, L::YS>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::bytes);
     if (e == cudaSuccess && L::CL > 8) e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     return e;
@@ -579,7 +586,7 @@ template <typename TC>
 static void line_x_config(wtd_ctx *c, cudaLaunchConfig_t &cfg, cudaLaunchAttribute *at, int ncl)
 {
     typedef LineCfg<TC> L;
-    typedef XSmem<TC, L::CL, L::TX, L::HPAD> SM;
+    typedef XSmem<TC, L::CL, L::TX, L::HPAD, L::YS> SM;
     memset(&cfg, 0, sizeof(cfg));
     cfg.gridDim = dim3((unsigned)(ncl * L::CL));
     cfg.blockDim = dim3(SM::XT);
@@ -604,7 +611,7 @@ static int line_launch_x(wtd_ctx *c, const StepArgs &a)
     X3Args xa;
     xa.s = a;
     xa.K = c->kbuf;
-    WTD_CU(cudaLaunchKernelEx(&cfg, k3_xline<TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD, L::CL, L::TX, L::HPAD>, xa,
+    WTD_CU(cudaLaunchKernelEx(&cfg, k3_xline<TY, TH, TC, WTD_NHIST, PASS, WTD_VAR, GRAD, L::CL, L::TX, L::HPAD, L::YS>, xa,
                               (const double2 *)c->tw, (const double *)c->ktab));
     WTD_LAUNCHED(c);
     return WTD_OK;
@@ -737,7 +744,7 @@ static int line_setup_t(wtd_ctx *c, int nsm)
         WTD_CU((line_x_attrs<TY, TH, TC, 0, false>()));
         line_x_config<TC>(c, cfg, at, 1);
         int ncl = 0;
-        if (cudaOccupancyMaxActiveClusters(&ncl, k3_xline<TY, TH, TC, WTD_NHIST, 0, WTD_VAR, false, L::CL, L::TX, L::HPAD>,
+        if (cudaOccupancyMaxActiveClusters(&ncl, k3_xline<TY, TH, TC, WTD_NHIST, 0, WTD_VAR, false, L::CL, L::TX, L::HPAD, L::YS>,
                                            &cfg) != cudaSuccess || ncl < 1) {
             cudaGetLastError();
             ncl = nsm / L::CL;

@@ -225,7 +225,7 @@ struct X3Args {
     const void *K;              /* K_yz of every state (TC complex, [2S][N]) */
 };
 
-template <typename TC, int CL, int TX_, int HPAD> struct XSmem {
+template <typename TC, int CL, int TX_, int HPAD, bool YSF> struct XSmem {
     typedef typename cplx<TC>::t C;
     static constexpr int TX = TX_;
     static constexpr int QC = WTD_L_NYZ / CL;
@@ -234,9 +234,9 @@ template <typename TC, int CL, int TX_, int HPAD> struct XSmem {
     static constexpr int HP = NX + HPAD;                                    /* padded line of H */
     static constexpr size_t tab = (sizeof(LineTab<TC, WTD_L_NMAX>) + 15) / 16 * 16;
     static constexpr size_t hs = (size_t)LINES * HP * sizeof(C);            /* H, then the update, per line */
-    /* the state's values per line (teams of TX > 1 threads; a thread that owns a whole line
-     * reads its values from L2/L1 instead) */
-    static constexpr bool YS = TX > 1;
+    /* the state's values per line, where chosen (YSF) and a team of TX > 1 threads shares a
+     * line; otherwise each thread reads its points' values from L2/L1 */
+    static constexpr bool YS = YSF && TX > 1;
     static constexpr size_t ys = YS ? hs : 0;
     static constexpr size_t scr = (size_t)LINES * team_scratch(NX, TX) * sizeof(C);
     static constexpr size_t red = 80 * sizeof(double);
@@ -311,21 +311,22 @@ __device__ __forceinline__ double cluster_collect(double *cred, int slot)
     return s;
 }
 
-template <typename TY, typename TH, typename TC, int NH, int PASS, bool VAR, bool GRAD, int CL, int TXT, int HPAD>
-__global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Args xa, const double2 *gtw, const double *gk)
+template <typename TY, typename TH, typename TC, int NH, int PASS, bool VAR, bool GRAD, int CL, int TXT, int HPAD, bool YSF>
+__global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD, YSF>::XT, 1) k3_xline(X3Args xa, const double2 *gtw, const double *gk)
 {
     namespace cg = cooperative_groups;
     typedef typename cplx<TC>::t C;
-    typedef XSmem<TC, CL, TXT, HPAD> SM;
+    typedef XSmem<TC, CL, TXT, HPAD, YSF> SM;
     constexpr int N = WTD_NUMEL, NYZ = WTD_L_NYZ, QC = SM::QC, XT = SM::XT, TX = SM::TX, HP = SM::HP;
     constexpr int n1 = NX / TX;
     const StepArgs &a = xa.s;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LineTab<TC, WTD_L_NMAX> &Tb = *(LineTab<TC, WTD_L_NMAX> *)smem_raw;
     static_assert(sizeof(TY) == sizeof(typename cplx<TC>::t), "states stored in the compute precision");
-    C *Hs = (C *)(smem_raw + SM::tab);                 /* [line][HP] */
-    C *Ysm = Hs + SM::LINES * HP;                      /* [line][HP]: the state of the iteration */
-    C *Scr = Ysm + SM::LINES * HP;                     /* [line][team scratch] */
+    /* every region at its XSmem offset: tab | hs | ys | scr | red | slabs */
+    C *Hs = (C *)(smem_raw + SM::tab);                                   /* [line][HP] */
+    C *Ysm = (C *)(smem_raw + SM::tab + SM::hs);                         /* [line][HP] (YS only) */
+    C *Scr = (C *)(smem_raw + SM::tab + SM::hs + SM::ys);                /* [line][team scratch] */
     double *red = (double *)(smem_raw + SM::tab + SM::hs + SM::ys + SM::scr);
     double *cs = (double *)(smem_raw + SM::base);        /* [NCS][NX][CP] coefficient slabs */
     constexpr int NCS = SM::NCS, CP = SM::CP, SL = NX * CP;
@@ -425,7 +426,7 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
         int eslot = 0;
         /* this line's state values into shared memory (read once from HBM; the local terms of
          * the other component's line read them there too), and K_yz into the line's H */
-#pragma unroll
+#pragma unroll 8
         for (int i = 0; i < n1; i++) {
             const int x = g + TX * i, p = x * NYZ + q;
             if (YS) {
@@ -529,23 +530,26 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
             cluster_post<CL>(e, red, cred, eslot);
         }
         /* the ABM inputs of this thread's points, loaded while the cluster sum of <H> completes:
-         * y and the first NRP history slots this pass reads */
+         * the first NRP history slots this pass reads (none where a thread owns more than 8
+         * points of a line: they would not stay in registers) */
         constexpr int NR = (PASS == 0) ? NH - 1 : (PASS == 1 ? 1 : 0);
-        constexpr int NRP = (PASS == 0) ? (sizeof(TH) == 8 ? 2 : 1) : (PASS == 1 ? 1 : 0);
+        constexpr int NRP = n1 > 8 ? 0 : (PASS == 0) ? (sizeof(TH) == 8 ? 2 : 1) : (PASS == 1 ? 1 : 0);
         auto ring = [&](int k) -> const TH * { return (const TH *)xa.s.slot[PASS == 1 ? NH - 2 : k]; };
-        TH frr[NRP > 0 ? NRP : 1][n1];
+        TH frr[NRP > 0 ? NRP : 1][NRP > 0 ? n1 : 1];
+        if constexpr (NRP > 0) {
 #pragma unroll
-        for (int i = 0; i < n1; i++) {
-            const size_t gi = fb + (size_t)(g + TX * i) * NYZ + q;
+            for (int i = 0; i < n1; i++) {
+                const size_t gi = fb + (size_t)(g + TX * i) * NYZ + q;
 #pragma unroll
-            for (int k = 0; k < NRP; k++) frr[k][i] = ld_stream(ring(k) + gi);
+                for (int k = 0; k < NRP; k++) frr[k][i] = ld_stream(ring(k) + gi);
+            }
         }
         if (haveH) {
             E = cluster_collect<CL>(cred, eslot) * WTD_DV;
             if (t == 0 && rank == 0) a.qpe[n] = E;
         }
         if (PASS == 3) {
-#pragma unroll
+#pragma unroll 2
             for (int i = 0; i < n1; i++) {
                 const int x = g + TX * i;
                 const size_t gi = fb + x * NYZ + q;
@@ -557,9 +561,11 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
             __syncthreads();
             continue;
         }
-        /* ---- ABM update of this thread's points, unnormalised into H ---- */
+        /* ---- ABM update of this thread's points, unnormalised into H (fully unrolled where
+         * the preloaded history words index frr by i; two points at a time otherwise) ---- */
         double nrm = 0.0;
-#pragma unroll
+        constexpr int ABMU = NRP > 0 ? n1 : 2;
+#pragma unroll ABMU
         for (int i = 0; i < n1; i++) {
             const int x = g + TX * i;
             const size_t gi = fb + x * NYZ + q;
@@ -567,7 +573,7 @@ __global__ void __launch_bounds__(XSmem<TC, CL, TXT, HPAD>::XT, 1) k3_xline(X3Ar
             const double2 y0 = make_double2((double)yc.x, (double)yc.y);
             double2 fr[NR > 0 ? NR : 1], fkg = make_double2(0.0, 0.0);
 #pragma unroll
-            for (int k = 0; k < NR; k++) fr[k] = to_d(k < NRP ? frr[k < NRP ? k : 0][i] : ld_stream(ring(k) + gi));
+            for (int k = 0; k < NR; k++) fr[k] = to_d(k < NRP ? frr[k < NRP ? k : 0][NRP > 0 ? i : 0] : ld_stream(ring(k) + gi));
             if (PASS == 0 && !haveH) fkg = to_d(ld_stream((const TH *)xa.s.slot[NH - 1] + gi));
             double2 fk = make_double2(0.0, 0.0);
             if (PASS != 2) {
