@@ -208,6 +208,33 @@ def energy_drift(name, nwf, d, precision, steps, dev):
     return dict(steps=steps, e0=e0, e_t=e1, drift_per_1000_steps=abs(e1 - e0) / abs(e0) * 1000.0 / steps), dens
 
 
+# nominal CUDA-core peaks of a B200 at its 1965 MHz maximum clock (148 SMs; 64 FP64 and 128
+# FP32 fused multiply-adds per SM per clock): the denominators of the flop rooflines below
+FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e-3
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e-3
+DENS_BLOCKS = ("nu", "rho_a", "tau_a", "j_a_x", "j_a_y", "j_a_z", "rho_b", "tau_b", "j_b_x", "j_b_y", "j_b_z")
+
+
+def dens_errs(dens, ref, n):
+    """relative L2 error per density block (the reference's 12-block layout; nu is complex)"""
+    out = {}
+    offs = [(0, 2 * n)] + [((2 + k) * n, (3 + k) * n) for k in range(10)]
+    for name, (a, b) in zip(DENS_BLOCKS, offs):
+        nr = float(np.linalg.norm(ref[a:b]))
+        if nr > 0:
+            out[name] = float(np.linalg.norm(dens[a:b] - ref[a:b]) / nr)
+    return out
+
+
+def fft_flops(proj):
+    """algorithmic flops of one qp-state-step's transforms: 5 N log2 N per complex transform,
+    14 transforms per component and step with variable mass (ASLDA), 4 with constant mass"""
+    import math
+    n = proj.numel
+    per = 14 if not proj.const_mass else 4
+    return 5.0 * n * math.log2(n) * per * 2
+
+
 def rho_err(dens, ref, n):
     """relative L2 error of (rho_a, rho_b)"""
     rho = np.concatenate([ref[2 * n:3 * n], ref[7 * n:8 * n]])
@@ -414,11 +441,18 @@ def c3_comparison(args, dev):
              "ms_blocks": t["ms_blocks"], "hbm_gbs_compulsory": (ba + bb) * nwf * args.c3_steps / (t["ms"] * 1e-3) / 1e9,
              "launches_per_block": t["launches"], "clocks": t["clocks"]}
         f["roofline_frac"] = f["hbm_gbs_compulsory"] / hbm
+        # the transforms' flops against the CUDA-core peak of the arithmetic precision (FP64 for
+        # the FP64 form, FP32 for the mixed forms): the C3 step is transform- and latency-bound
+        tf = fft_flops(proj) * f["value"] / 1e12
+        fpk = FP64_PEAK_TFLOPS if prec == 0 else FP32_PEAK_TFLOPS
+        f["flops"] = {"alg_flops_per_state_step": fft_flops(proj), "achieved_tflops": tf, "peak_tflops": fpk,
+                      "peak_source": "nominal (148 SMs x FMA/clk x 1965 MHz)", "frac": tf / fpk}
         if label == "fp64":
             dens64 = dens
         else:
             f["speedup_vs_fp64"] = out["forms"]["fp64"]["value"] and f["value"] / out["forms"]["fp64"]["value"]
             f["density_rel_l2_err_vs_fp64"] = rho_err(dens, dens64, proj.numel)
+            f["density_rel_l2_err_vs_fp64_by_block"] = dens_errs(dens, dens64, proj.numel)
         out["forms"][label] = f
         torch.cuda.empty_cache()
     out["peak_gbs"] = hbm
@@ -731,6 +765,7 @@ def main():
             forms[label] = {"value": nwf_total * args.steps / (m["ms"] * 1e-3), "ms_blocks": m["ms_blocks"],
                             "speedup_vs_fp64": f["ms"] / m["ms"],
                             "density_rel_l2_err_vs_fp64": rho_err(m["dens"], f["dens"], n),
+                            "density_rel_l2_err_vs_fp64_by_block": dens_errs(m["dens"], f["dens"], n),
                             "energy_rel_err_vs_fp64": float(abs(total_energy(m["energy"]) - total_energy(f["energy"])) /
                                                             abs(total_energy(f["energy"]))),
                             "ms_pass_a": m["ms_a"], "ms_pass_b": m["ms_b"]}
