@@ -71,6 +71,7 @@ struct wtd_ctx {
     double qfsw;
     double *dqf, *qfld;
     int sstride;                /* density-slot words per CTA: 12 N, 16 N with quantum friction */
+    int sdg;                    /* state chunks of the staged density kernel (staged_dens_chunks) */
 };
 
 static void adj_release(wtd_ctx *c);
@@ -404,20 +405,30 @@ static int st_round(wtd_ctx *c)
     return st_load(c);
 }
 
+/* state chunks of the staged density kernel: WTD_DP_T-point tiles times chunks make one full
+ * wave of resident CTAs, at most one chunk per slot of the context.  Computed once per context
+ * (wtd_create); the densities' summation order follows the chunks, so it is fixed for a given
+ * GPU model and build (bitwise reproducible run to run), not across GPU models. */
+static int staged_dens_chunks(wtd_ctx *c, int *G)
+{
+    constexpr int N = WTD_NUMEL;
+    const int tiles = (N + WTD_DP_T - 1) / WTD_DP_T;
+    int nsm = 0, per_sm = 0;
+    WTD_CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev));
+    WTD_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dens_points, WTD_DP_T, 0));
+    int g = nsm * (per_sm > 0 ? per_sm : 1) / tiles;
+    if (g > c->grid) g = c->grid;
+    if (g > c->S) g = c->S;
+    *G = g < 1 ? 1 : g;
+    return WTD_OK;
+}
+
 static int staged_densities(wtd_ctx *c, bool grads)
 {
     constexpr int N = WTD_NUMEL;
     const int S = c->S;
-    /* parallel over points: WTD_DP_T-point tiles times state chunks, as many chunks as make one
-     * full wave of resident CTAs, at most one per slot of the context */
     const int tiles = (N + WTD_DP_T - 1) / WTD_DP_T;
-    int nsm = 0, per_sm = 1;
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dens_points, WTD_DP_T, 0);
-    int G = nsm * per_sm / tiles;
-    if (G > c->grid) G = c->grid;
-    if (G > S) G = S;
-    if (G < 1) G = 1;
+    const int G = c->sdg > 0 ? c->sdg : 1;
     k_dens_points<<<dim3(tiles, G), WTD_DP_T, 0, c->st>>>(S, G, st_y(c), c->ddx, c->ddy, c->ddz, c->dlap, c->occ,
                                                           c->kp2, c->wcnt, c->dslot, grads ? 1 : 0);
     WTD_LAUNCHED(c);
@@ -941,6 +952,7 @@ int wtd_create(wtd_ctx **out, int nwf, int precision, int device)
     int per_sm = WTD_BIG ? 2 : occupancy_per_sm(c);
     c->grid = nsm * per_sm;
     if (c->grid > nwf) c->grid = nwf;
+    if (c->staged && staged_dens_chunks(c, &c->sdg) != WTD_OK) { cudaGetLastError(); free(c); return WTD_ERR_CUDA; }
     cudaError_t e = cudaSuccess;
 #define ALLOC(p, bytes) if (e == cudaSuccess) e = cudaMalloc((void **)&(p), (bytes))
     ALLOC(c->y, c->ysz);

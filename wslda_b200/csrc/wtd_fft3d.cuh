@@ -156,10 +156,16 @@ static int big_derivs(double2 *in, int nf, double2 *lap, double2 *dx, double2 *d
 #define WTD_PXS_CAP (2048 / (NX) >= 32 ? 32 : 2048 / (NX) >= 16 ? 16 : 2048 / (NX) >= 8 ? 8 : 4)
 #define WTD_PXS (WTD_NYZ % WTD_PXS_CAP == 0 ? WTD_PXS_CAP : WTD_PX)
 
-/* 4 CTAs per SM (at most 64 registers a thread): the plane FFT stages are latency-bound, and
- * the register file otherwise admits 3 */
+/* CTAs per SM asked of the register allocator for the plane kernel: 4 (at most 64 registers a
+ * thread; the plane FFT stages are latency-bound, and the register file otherwise admits 3)
+ * where 4 CTAs' shared memory fits an SM (228 KB, 1 KB reserved per CTA), else as many as fit */
+template <class GP> struct SepPlanesMinB {
+    static constexpr size_t smem = 2 * (size_t)GP::padded * sizeof(double2) + GP::twtotal * sizeof(double2) + sizeof(KTab<GP>);
+    static constexpr size_t per = smem + 1024, sm = 233472;
+    static constexpr int value = 4 * per <= sm ? 4 : 3 * per <= sm ? 3 : 2 * per <= sm ? 2 : 1;
+};
 template <class GP>
-__global__ void __launch_bounds__(WTD_SEP_NT, 4) k_sep_planes(const double2 *__restrict__ in, double2 *lap, double2 *dy,
+__global__ void __launch_bounds__(WTD_SEP_NT, SepPlanesMinB<GP>::value) k_sep_planes(const double2 *__restrict__ in, double2 *lap, double2 *dy,
                                                           double2 *dz, const double *wa, const double *wb, int nfa,
                                                           const double2 *gtw_yz, const double *gk)
 {
