@@ -517,6 +517,15 @@ __global__ void wtd_energy_kernel(int it, wslda_density Dn, wslda_potential P, d
 #define wtd_energy_kernel tdwslda_compute_energy
 #endif
 
+/* threads per CTA of the potentials kernel: the built-in functionals are a few hundred FP64
+ * operations per point on a lattice of a few thousand points, so one warp per CTA spreads them
+ * over more SMs; the user's CUSTOMEDF kernel keeps the reference's launch shape */
+#if FUNCTIONAL == CUSTOMEDF
+#define WTD_POT_THREADS 128
+#else
+#define WTD_POT_THREADS 32
+#endif
+
 /* external-field energies, particle number and L_z integrands
  * (pca_kernels.cu:121-209; cpca_kernels.cu:121-209; tdwslda_energy_generic.h:40-92) */
 __global__ void wtd_energy_ext_kernel(int it, wslda_density Dn, wslda_potential P, double *e)
