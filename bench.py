@@ -545,32 +545,48 @@ def c5_scale(args, dev):
     # measurement normalises each state
     import ctypes
     seed = P.config_seed(name)
-    r = TDRun(name, nwf, precision=2, device=dev)
-    sp = ctypes.c_void_p()
-    r._check(r.lib.wtd_device_pointers(r.h, ctypes.byref(sp), None, None))
-    g = torch.Generator(device="cuda")
-    g.manual_seed(seed)
-    n2 = 2 * nwf * proj.numel
-    chunk = 1 << 27
-    for o in range(0, n2, chunk):
-        m = min(chunk, n2 - o)
-        z = torch.randn(2 * m, device="cuda", dtype=torch.float32, generator=g)
-        r.lib.memcopy_gpu2gpu(ctypes.c_void_p(z.data_ptr()), ctypes.c_void_p(sp.value + 8 * o), ctypes.c_size_t(8 * m))
-        del z
-    torch.cuda.synchronize()
-    r.setup_fields(P.make_potentials(proj), P.make_occupations(nwf), proj.params, P.make_extra(proj, seed))
-    r.initial_measurement()
-    r.steps(args.warmup)
-    r.sync()
-    stream = torch.cuda.ExternalStream(r.stream())
-    t = timed_blocks(r, stream, args.c5_steps, args.blocks, dev, 1)
-    r.close()
-    ba, bb = pass_bytes(proj, 2)
     hbm, _ = peaks()
-    out.update({"value": nwf * args.c5_steps / (t["ms"] * 1e-3), "ms_per_step": t["ms"] / args.c5_steps,
-                "ms_blocks": t["ms_blocks"], "hbm_gbs_compulsory": (ba + bb) * nwf * args.c5_steps / (t["ms"] * 1e-3) / 1e9,
-                "clocks": t["clocks"]})
-    out["roofline_frac"] = out["hbm_gbs_compulsory"] / hbm
+
+    def timed_form(prec, ns):
+        r = TDRun(name, ns, precision=prec, device=dev)
+        sp = ctypes.c_void_p()
+        r._check(r.lib.wtd_device_pointers(r.h, ctypes.byref(sp), None, None))
+        g = torch.Generator(device="cuda")
+        g.manual_seed(seed)
+        n2 = 2 * ns * proj.numel
+        chunk = 1 << 27
+        dt_, eb = (torch.float32, 8) if prec else (torch.float64, 16)
+        for o in range(0, n2, chunk):
+            m = min(chunk, n2 - o)
+            z = torch.randn(2 * m, device="cuda", dtype=dt_, generator=g)
+            r.lib.memcopy_gpu2gpu(ctypes.c_void_p(z.data_ptr()), ctypes.c_void_p(sp.value + eb * o), ctypes.c_size_t(eb * m))
+            del z
+        torch.cuda.synchronize()
+        r.setup_fields(P.make_potentials(proj), P.make_occupations(ns), proj.params, P.make_extra(proj, seed))
+        r.initial_measurement()
+        r.steps(args.warmup)
+        r.sync()
+        stream = torch.cuda.ExternalStream(r.stream())
+        t = timed_blocks(r, stream, args.c5_steps, args.blocks, dev, 1)
+        r.close()
+        torch.cuda.empty_cache()
+        ba, bb = pass_bytes(proj, prec)
+        res = {"states": ns, "value": ns * args.c5_steps / (t["ms"] * 1e-3), "ms_per_step": t["ms"] / args.c5_steps,
+               "ms_blocks": t["ms_blocks"], "hbm_gbs_compulsory": (ba + bb) * ns * args.c5_steps / (t["ms"] * 1e-3) / 1e9,
+               "clocks": t["clocks"]}
+        res["roofline_frac"] = res["hbm_gbs_compulsory"] / hbm
+        return res
+
+    f32 = timed_form(2, nwf)
+    f32.pop("states")
+    out.update(f32)
+    # the FP64 form on the same GPU, at the state count its resident arrays allow (the staged
+    # path: states, ring and the derivative arrays); qp-state*steps/s is per state, so the two
+    # rates compare directly
+    if args.c5_fp64_nwf > 0:
+        f64 = timed_form(0, args.c5_fp64_nwf)
+        out["fp64"] = f64
+        out["speedup_vs_fp64"] = out["value"] / f64["value"]
     # accuracy against FP64 on a subset of the workload
     ns = args.c5_err_nwf
     pe, de = make_inputs(name, ns)
@@ -665,6 +681,7 @@ def main():
     ap.add_argument("--c5-steps", type=int, default=3)
     ap.add_argument("--c5-err-nwf", type=int, default=256)
     ap.add_argument("--c5-err-steps", type=int, default=20)
+    ap.add_argument("--c5-fp64-nwf", type=int, default=2000, help="states of the C5 FP64 comparison (0: skip)")
     ap.add_argument("--probe", type=int, default=-1, choices=[-1, 0, 1, 2],
                     help="time one precision form (0 FP64, 1 mixed H64, 2 mixed H32) of the workload for --steps "
                          "steps after --warmup, print one short JSON line and exit (the profiling case)")
