@@ -302,11 +302,10 @@ static int functional(wtd_ctx *c, int it)
     constexpr int N = WTD_NUMEL;
     wslda_density D = convert_into_wslda_density(c->dens, N);
     wslda_potential P = convert_into_wslda_potential(c->pots, N, NULL);
-    int pb = (N + 127) / 128;
     wtd_potentials_kernel<<<(N + WTD_POT_THREADS - 1) / WTD_POT_THREADS, WTD_POT_THREADS, 0, c->st>>>(it, D, P, 1.0);
     WTD_LAUNCHED(c);
 #ifdef ENABLE_MODIFY_POTENTIALS
-    modify_potentials<<<pb, 128, 0, c->st>>>(it, D, P);
+    modify_potentials<<<(N + 127) / 128, 128, 0, c->st>>>(it, D, P);
     WTD_LAUNCHED(c);
 #endif
     return WTD_OK;
